@@ -1,0 +1,331 @@
+"""Benchmark: 4-clique counting on the degree-oriented R-MAT scale-22, edge-factor-16 graph.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one exact 4-clique count (kautomine/four_clique.cc schedule semantics) over the
+whole graph.  The metric is embeddings/s = (NumExtensions + count) / time, NumExtensions
+being the reference engine's own extension counter (engine.cc:924) for that schedule.
+
+* value: device time (CUDA events around the counting launches, graph resident in HBM);
+  the graph (256 MB of adjacency + 19 MB of offsets) is larger than the 126 MB L2, so no
+  flush is needed between steps.
+* e2e: the C-ABI path a user takes with host buffers: upload the oriented .dgraph edge list
+  from pinned memory, device CSR build, count, copy the result back.
+* roofline: algorithmic bytes of the dominant kernel (instrumented run) / its measured time.
+* cpu_baseline: the reference's own kautomine four_clique app (oracle/_ref, compiled from the
+  reference's sources) on a label-restricted slice of the start vertices, all host threads.
+* --impl reference: the same reference binary as the timed arm, on the same slice.
+* N > 1 (torchrun): replicas only; each rank counts the same graph on its own GPU.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE, EDGE_FACTOR, SEED = 22, 16, 1
+RMAT_ABC = (0.57, 0.19, 0.19)
+APP = "kautomine_four_clique"
+SAMPLE_MOD = 32      # CPU sample: start vertices with v0 % 32 == 0 (one label class of 32)
+METRIC = "embeddings/s (4-clique, exact uint64 count)"
+WORKLOAD = "4-clique count, R-MAT scale 22 ef 16 (a,b,c)=(0.57,0.19,0.19) seed 1, degree-oriented DAG"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(gpus):
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def max_over_ranks(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world, device):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier(device_ids=[device])
+    torch.cuda.synchronize()
+
+
+# ------------------------------------------------------------------------------ reference / CPU
+def labelled_oriented_dgraph(g, tmpdir):
+    """Writes the oriented graph as a labelled .dgraph (labels v % SAMPLE_MOD) for the sampled
+    reference driver."""
+    import numpy as np
+    n = g.num_vertices
+    path = os.path.join(tmpdir, "k_oriented_labeled.dgraph")
+    g.write_dgraph(path, labels=(np.arange(n, dtype=np.uint64) % SAMPLE_MOD).astype(np.uint32))
+    return path
+
+
+def run_reference_sample(dgraph, runs):
+    """The reference's own kautomine four_clique (apply + engine, compiled unmodified) over the
+    start vertices of label class 0; returns (per-run seconds, embeddings per run, kind, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    cores = os.cpu_count() or 1
+    exe = os.path.join(orc.REF_DIR, "sample_" + APP)
+    if os.path.exists(exe):
+        counts, avg_ms, ext = orc.run_reference(APP, dgraph, threads=-1, runs=runs, label=0, timeout=3000)
+        per_run_ext = ext // runs
+        threads = max(1, cores - 2)  # the reference caps compute threads at cores - 2 (distributed_application.cc:80)
+        return avg_ms / 1000.0, per_run_ext + counts[0], "reference", threads
+    # the oracle port (C restatement) when the reference binaries are not present
+    n, pairs, _ = orc.read_dgraph(dgraph)
+    off, adj = orc.csr(pairs, n)
+    t0 = time.time()
+    for _ in range(runs):
+        counts, ext, _ = orc.count(APP, off, adj, v0_mod=SAMPLE_MOD, v0_rem=0, threads=cores)
+    dt = (time.time() - t0) / runs
+    return dt, ext + counts[0], "port", cores
+
+
+# ------------------------------------------------------------------------------ main arms
+def ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    from openkhuzdulgraph_b200 import khz
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = khz.Context(local)
+    a, b, c = RMAT_ABC
+    sym = ctx.generate_rmat(SCALE, EDGE_FACTOR, a, b, c, SEED)
+    g = sym.orient()
+    gi = g.info()
+    n, m = gi.num_vertices, gi.num_entries
+    sym_info = sym.info()
+    sym.free()
+
+    # instrumented run (untimed): algorithmic bytes per phase, NumExtensions, count
+    ctx.set_config(want_algo_bytes=1)
+    ref_counts, st_stats = ctx.count(g, APP)
+    ctx.set_config(want_algo_bytes=0)
+    embeddings = st_stats.num_extensions + ref_counts[0]
+
+    stream = torch.cuda.Stream(dev)
+    sptr = stream.cuda_stream
+    for _ in range(args.warmup):
+        counts, st = ctx.count(g, APP, stream=sptr)
+        assert counts == ref_counts
+    barrier(world, local)
+    phase_ms = [0.0] * 4
+    launches = 0
+    step_ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            counts, st = ctx.count(g, APP, stream=sptr)
+            assert counts == ref_counts and st.num_extensions == st_stats.num_extensions
+            step_ms.append(st.kernel_ms)
+            launches += st.launches
+            for p in range(4):
+                phase_ms[p] += st.phase_ms[p]
+    barrier(world, local)
+    total_ms = max_over_ranks(sum(step_ms), world, local)
+    ms_per_step = total_ms / args.steps
+    value = embeddings * world / (ms_per_step / 1000.0)
+
+    # dominant kernel and its roofline
+    dom = max(range(4), key=lambda p: phase_ms[p])
+    dom_ms = phase_ms[dom] / args.steps
+    dom_bytes = st_stats.phase_bytes[dom]
+    peak, peak_kind = peaks()
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get(khz.Stats.PHASES[dom])
+
+    # e2e: oriented .dgraph edge list in pinned host memory -> C ABI -> count -> host
+    off_h, adj_h = g.export_csr()
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off_h).astype(np.int64))
+    pairs = torch.from_numpy(np.stack([src, adj_h], axis=1).reshape(-1).view(np.int32)).pin_memory()
+    del src
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g2 = ctx.graph_from_edges(pairs, n, stream=sptr)
+        c2, st2 = ctx.count(g2, APP, stream=sptr)
+        g2.free()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        assert c2 == ref_counts
+        if i >= args.warmup:
+            e2e_ms.append((t1 - t0) * 1000.0)
+    e2e_total = max_over_ranks(sum(e2e_ms), world, local)
+    e2e_value = embeddings * world / (e2e_total / args.steps / 1000.0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        with tempfile.TemporaryDirectory() as td:
+            path = labelled_oriented_dgraph(g, td)
+            secs, emb, kind, cores = run_reference_sample(path, runs=1)
+        cpu = {"value": emb / secs, "unit": "embeddings/s", "cores": cores, "kind": kind,
+               "sample": "start vertices v0 %% %d == 0 of the same oriented graph (%d embeddings, %.1f s)"
+                         % (SAMPLE_MOD, emb, secs)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "embeddings/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic (device R-MAT generator)",
+            "config": {"workload": WORKLOAD, "vertices": n, "oriented_edges": m,
+                       "undirected_edges": sym_info.num_entries // 2, "max_out_degree": gi.max_degree,
+                       "count": ref_counts[0], "num_extensions": st_stats.num_extensions,
+                       "embeddings_per_step": embeddings, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs (275 MB CSR) larger than L2; no flush"},
+            "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": int(pairs.numel() * 4),
+                    "d2h_bytes_per_step": 8 * 8, "ms_per_step": e2e_total / args.steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": khz.Stats.PHASES[dom], "kernel_ms": dom_ms,
+                         "algo_bytes_per_launch": dom_bytes},
+            "phase_ms_per_step": [x / args.steps for x in phase_ms],
+            "phase_algo_bytes": list(st_stats.phase_bytes),
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def reference_arm(args, rank, world, local):
+    if rank != 0:
+        return
+    from openkhuzdulgraph_b200 import khz
+    import torch
+    torch.cuda.set_device(local)
+    ctx = khz.Context(local)
+    a, b, c = RMAT_ABC
+    sym = ctx.generate_rmat(SCALE, EDGE_FACTOR, a, b, c, SEED)
+    g = sym.orient()
+    sym.free()
+    with tempfile.TemporaryDirectory() as td:
+        path = labelled_oriented_dgraph(g, td)
+        ctx.close()
+        secs, emb, kind, cores = run_reference_sample(path, runs=args.steps)
+    value = emb / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "embeddings/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": 0, "ms_per_step": secs * 1000.0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": "v0 %% %d == 0" % SAMPLE_MOD},
+            "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": cores, "kind": kind,
+                             "sample": "start vertices v0 %% %d == 0 (%d embeddings per step)" % (SAMPLE_MOD, emb)},
+            "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        # the reference arm is a CPU run on rank 0; other ranks exit without work
+        rank = int(os.environ.get("RANK", "0"))
+        reference_arm(args, rank, 1, int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, rank, world, local)
+        else:
+            ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,186 @@
+/*
+ * khz.h — C ABI of the B200 embedding-extension engine (libkhz_b200.so).
+ *
+ * Plain C: pointers, sizes and opaque handles only.  Every entry point returns a
+ * khz_status and never aborts; khz_last_error_string() describes the last failure
+ * of the calling thread.  Streams are passed as void* (a cudaStream_t, NULL for the
+ * legacy default stream).
+ *
+ * Each declaration names the reference interface it replaces (paths relative to
+ * the AmadeusChan/OpenKhuzdulGraph tree).
+ */
+#ifndef KHZ_H
+#define KHZ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KHZ_ABI_VERSION 1
+
+/* Error codes.  Replaces the reference's assert()/exit(-1) failure paths
+ * (e.g. distributed_application.cc:281-282, engine.cc:53-55, kautomine/triangle.cc:112-119). */
+typedef enum khz_status {
+    KHZ_OK = 0,
+    KHZ_ERR_ARG = 1,      /* bad handle, id or size: rejected before any launch */
+    KHZ_ERR_OOM = 2,      /* device or pinned allocation failed */
+    KHZ_ERR_OVERFLOW = 3, /* a device-side capacity check fired (result dropped) */
+    KHZ_ERR_TIMEOUT = 4,  /* a bounded device or host wait ran out */
+    KHZ_ERR_CUDA = 5,     /* a CUDA runtime call failed */
+    KHZ_ERR_FORMAT = 6,   /* input graph violates the .dgraph contract */
+    KHZ_ERR_BUSY = 7,     /* serving queue full / ticket not finished */
+    KHZ_ERR_NOT_FOUND = 8
+} khz_status;
+
+/* Pattern applications; the numbering is shared with the oracle.
+ * 0-7 are the reference's apps, 8-11 are schedules written in the same idioms. */
+typedef enum khz_app_id {
+    KHZ_KAUTO_TRIANGLE = 0,        /* kautomine/triangle.cc:58-121 */
+    KHZ_KAUTO_4CLIQUE = 1,         /* kautomine/four_clique.cc:58-153 */
+    KHZ_KAUTO_5CLIQUE = 2,         /* kautomine/five_clique.cc:58-186 */
+    KHZ_KAUTO_3MOTIF = 3,          /* kautomine/three_motif.cc:40-44,59-138 (2 counts) */
+    KHZ_KGPI_TRIANGLE = 4,         /* kgraphpi/triangle.cc:53-122 */
+    KHZ_KGPI_4CLIQUE = 5,          /* kgraphpi/four_clique.cc:53-159 */
+    KHZ_KGPI_5CLIQUE = 6,          /* kgraphpi/five_clique.cc:53-195 */
+    KHZ_KGPI_3MOTIF = 7,           /* kgraphpi/three_motif.cc:52-174 (2 counts) */
+    KHZ_KGPI_4CYCLE = 8,           /* 4-cycle, kgraphpi idiom (edge-induced) */
+    KHZ_KGPI_HOUSE = 9,            /* house, kgraphpi idiom (edge-induced) */
+    KHZ_KGPI_TAILED_TRIANGLE = 10, /* tailed triangle, kgraphpi idiom (edge-induced) */
+    KHZ_KAUTO_4MOTIF = 11,         /* vertex-induced 4-motifs, kautomine idiom (6 counts) */
+    KHZ_NUM_APPS = 12
+} khz_app_id;
+
+#define KHZ_MAX_COUNTS 6
+
+typedef struct khz_ctx khz_ctx;
+typedef uint32_t khz_graph; /* 0 is never a valid handle */
+
+/* graph flags */
+#define KHZ_EDGES_ON_DEVICE 0x1u /* the pairs pointer is device memory */
+#define KHZ_ORIENT 0x2u          /* store the degree-oriented DAG instead of the symmetric CSR */
+#define KHZ_UNCHECKED 0x4u       /* skip the sortedness/range validation pass */
+
+/* engine choice (khz_config.engine) */
+#define KHZ_ENGINE_AUTO 0
+#define KHZ_ENGINE_DFS 1     /* per-warp DFS over the schedule with warp-cooperative set ops */
+#define KHZ_ENGINE_BITMAP 2  /* clique apps: local-subgraph bitmap engine on the oriented DAG */
+
+typedef struct khz_graph_info {
+    uint32_t num_vertices;
+    uint32_t max_degree;
+    uint64_t num_entries;  /* CSR entries: 2|E| symmetric, |E| oriented */
+    int32_t oriented;
+    int32_t reserved;
+    const uint64_t *d_offsets; /* device, num_vertices + 1 */
+    const uint32_t *d_adj;     /* device, num_entries (+ 4 padding entries) */
+    uint64_t device_bytes;     /* HBM held by this graph */
+} khz_graph_info;
+
+typedef struct khz_stats {
+    uint64_t num_extensions; /* the engine's NumExtensions (engine.cc:924) for the app's schedule */
+    uint64_t algo_bytes;     /* 4 * sum (|A|+|B|+|A op B|) of the schedule's set ops (when requested) */
+    double kernel_ms;        /* device time of the counting launches (CUDA events) */
+    uint32_t engine;         /* KHZ_ENGINE_* actually used */
+    uint32_t launches;       /* kernels launched by the call */
+    /* per phase: 0 bitmap warp tier, 1 bitmap mid block tier, 2 bitmap large block tier, 3 DFS engine */
+    double phase_ms[4];       /* device time of the phase's kernel (CUDA events; 0 if not run) */
+    uint64_t phase_bytes[4];  /* algorithmic bytes of the phase (instrumented runs only) */
+    uint32_t phase_launches[4];
+} khz_stats;
+
+typedef struct khz_config {
+    int32_t engine;            /* KHZ_ENGINE_*; AUTO picks per app and graph */
+    int32_t want_algo_bytes;   /* 1: run the instrumented variant that also sums algorithmic bytes */
+    int32_t dfs_warps_per_sm;  /* resident warps per SM for the DFS engine (0 = default) */
+    int32_t dfs_chunk;         /* level-1 candidates claimed per warp per grab (0 = default) */
+    int32_t bitmap_warp_max;   /* largest out-degree served by one warp in the bitmap engine (32|64) */
+    int32_t bitmap_block_warps;/* warps per block of the bitmap engine's block tier */
+    int32_t reserved[10];
+} khz_config;
+
+/* ---- context ---------------------------------------------------------------------- */
+/* Replaces DistributedSys::init_distributed_sys + the engine's buffer setup
+ * (distributed_sys.cc:11-35, engine.cc:1152-1244): one context owns all device memory. */
+khz_status khz_ctx_create(int device, khz_ctx **out);
+khz_status khz_ctx_destroy(khz_ctx *ctx);
+khz_status khz_ctx_set_config(khz_ctx *ctx, const khz_config *cfg);
+khz_status khz_ctx_get_config(khz_ctx *ctx, khz_config *cfg);
+const char *khz_last_error_string(void);
+int khz_abi_version(void);
+
+/* ---- graphs ----------------------------------------------------------------------- */
+/* Sorted (src,dst) edge list -> HBM-resident CSR built on the device.  Replaces
+ * CSRGraphLoader::load_graph / construct_csr_format_for_empty (graph_loader.h:154-201,
+ * 210-499) and the distributed loader's CSR build (graph_loader.h:621-703).  pairs holds
+ * m packed (src, dst) uint32 pairs sorted by (src, dst) without duplicates or self-loops,
+ * exactly the .dgraph edge section (graph_loader.h:31-42). */
+khz_status khz_graph_from_edges(khz_ctx *ctx, const uint32_t *pairs, uint64_t m, uint32_t n,
+                                uint32_t flags, khz_graph *out, void *stream);
+/* Reads a .dgraph file (header, optional node labels, edges) and builds the CSR.
+ * Replaces JointHashBasedNumaAwareDistGraphLoader::load_graphs (graph_loader.h:706-961). */
+khz_status khz_graph_load_dgraph(khz_ctx *ctx, const char *path, uint32_t flags, khz_graph *out);
+/* Degree orientation on the device: rank by (degree, id), keep rank(u) < rank(v), sorted
+ * out-lists.  Replaces toolkits/to_oriented_dataset_converter.cc:27-124. */
+khz_status khz_graph_orient(khz_ctx *ctx, khz_graph in, khz_graph *out, void *stream);
+/* Device R-MAT generator: raw edges -> drop self-loops -> canonical dedupe -> drop isolated
+ * vertices with order-preserving compaction -> symmetric CSR.  Follows the dataset pipeline
+ * datasets/live_journal/standardize.cc:66-111 + toolkits/converter.cc:151-268. */
+khz_status khz_graph_generate_rmat(khz_ctx *ctx, int scale, int edge_factor, double a, double b,
+                                   double c, uint64_t seed, uint32_t flags, khz_graph *out, void *stream);
+khz_status khz_graph_info_get(khz_ctx *ctx, khz_graph g, khz_graph_info *info);
+/* Copies the CSR to host memory (offsets: n+1 uint64, adj: num_entries uint32). */
+khz_status khz_graph_export_csr(khz_ctx *ctx, khz_graph g, uint64_t *offsets, uint32_t *adj);
+/* Writes the graph as a .dgraph file (symmetric or oriented, as stored); labels may be NULL. */
+khz_status khz_graph_write_dgraph(khz_ctx *ctx, khz_graph g, const char *path, const uint32_t *labels);
+/* Frees the graph's HBM.  Replaces destroy_graphs (graph_loader.h:963-974). */
+khz_status khz_graph_free(khz_ctx *ctx, khz_graph g);
+
+/* ---- counting --------------------------------------------------------------------- */
+/* One application on one graph: replaces `count->clear(); app->run(); count->evaluate()`
+ * (kautomine/triangle.cc:211-216, distributed_application.cc:259-356, engine.h:615-673).
+ * counts receives khz_app_num_counts(app) uint64 values, already divided by the app's
+ * multiplicities.  Blocks until the result is on the host. */
+khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts, khz_stats *stats,
+                     void *stream);
+/* Enqueues the same work without waiting: d_out (device, >= 8 uint64) receives
+ * [0..5] counts, [6] NumExtensions, [7] algorithmic bytes (0 unless configured). */
+khz_status khz_count_async(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *d_out, void *stream);
+int khz_app_num_counts(khz_app_id app);
+/* mirrors the reference's `multiplicities[]` tables (kautomine/three_motif.cc:44) */
+int khz_app_multiplicity(khz_app_id app, int pattern);
+
+/* ---- batched counting (many graphs / apps in one persistent launch) --------------- */
+typedef struct khz_job {
+    khz_graph graph;
+    int32_t app;
+    int32_t reserved;
+} khz_job;
+/* counts: n_jobs * KHZ_MAX_COUNTS uint64 (row per job); num_ext: n_jobs uint64 or NULL. */
+khz_status khz_count_batch(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64_t *counts,
+                           uint64_t *num_ext, khz_stats *stats, void *stream);
+
+/* ---- VertexSet algebra as a batch (test / tool entry) ----------------------------- */
+/* VertexSet::intersect_with / subtracted_by / intersect_and_count / bounded_* and the
+ * trims (vertex_set.cc:20-184, utilities.h:64-86) over n_pairs independent pairs of
+ * sorted strictly increasing uint32 lists, all buffers on the device.  Pair i uses
+ * a[a_off[i] .. a_off[i+1]) and b[b_off[i] .. b_off[i+1]); results go to
+ * out[a_off[i] ..] (capacity |A_i|), out_len[i] receives the size (or count).
+ * bound[i] is the upper bound of the bounded ops (ignored otherwise; may be NULL). */
+#define KHZ_SETOP_INTERSECT 0
+#define KHZ_SETOP_SUBTRACT 1
+#define KHZ_SETOP_INTERSECT_COUNT 2
+#define KHZ_SETOP_BOUNDED_INTERSECT 3
+#define KHZ_SETOP_BOUNDED_SUBTRACT 4
+#define KHZ_SETOP_TRIM 5               /* trim_v_list(A, bound): #elements < bound */
+#define KHZ_SETOP_TRIM_LOWER_BOUND 6   /* trim_v_list_lower_bound(A, bound): #elements <= bound */
+khz_status khz_set_op_batch(int op, const uint64_t *a_off, const uint32_t *a, const uint64_t *b_off,
+                            const uint32_t *b, const uint32_t *bound, uint32_t *out, uint32_t *out_len,
+                            uint32_t n_pairs, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

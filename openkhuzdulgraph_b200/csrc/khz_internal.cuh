@@ -1,0 +1,149 @@
+// Internal types shared by the engine's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "khz.h"
+
+namespace khz {
+
+constexpr int kMaxK = 5;       // MAX_PATTERN_SIZE (engine.h:23)
+constexpr int kNumSlots = 6;   // per-warp materialised sets: 1..3 level prefixes, 4 extra, 5 temp
+constexpr uint32_t kAdjPad = 8;  // padding entries after every adjacency array (vector loads)
+
+// ---------------------------------------------------------------------------------
+// Schedule IR.  Each reference apply() level becomes one KhzLevel: the candidate set of
+// vertex v_l is `base OP1 N(x1) OP2 N(x2)` (base = N(v_a) or a materialised prefix), the
+// filters are the generated code's `v > v_a` / `v != v_a` tests, and the last level is
+// one or two counting terms (compute-fused apps, kautomine/three_motif.cc:87-127).
+// ---------------------------------------------------------------------------------
+enum : int8_t { BASE_NBR = 0, BASE_SLOT = 1 };
+enum : int8_t { OP_NONE = 0, OP_AND = 1, OP_SUB = 2 };
+
+struct SetExpr {
+    int8_t base_kind;
+    int8_t base_arg;   // vertex index (BASE_NBR) or slot id (BASE_SLOT)
+    int8_t op[2];
+    int8_t op_arg[2];  // vertex index b of N(v_b)
+};
+
+struct Term {
+    SetExpr set;
+    uint8_t gt_mask;   // keep x > v_a for every bit a
+    uint8_t ne_mask;   // keep x != v_a for every bit a
+    int8_t guard_lo;   // evaluate only when v[guard_lo] < v[guard_hi] (-1: always)
+    int8_t guard_hi;
+    int8_t counter;    // last level: output counter index
+    int8_t pad[3];
+};
+
+struct Level {
+    Term t;            // enumeration term of this level (counter unused)
+    int8_t has_extra;  // compute `extra` into slot 4 on entry (a cached object)
+    int8_t finalized;  // children are executed in place: no NumExtensions (engine.cc:1441-1452)
+    int8_t pad[2];
+    SetExpr extra;
+};
+
+struct Plan {
+    int8_t k;          // pattern size; levels 1..k-2 enumerate, level k-1 counts
+    int8_t num_terms;  // counting terms at level k-1 (1 or 2)
+    int8_t pad[2];
+    Level lv[kMaxK];   // lv[1..k-2]; lv[1] must enumerate N(v0) (the DFS unit is one CSR entry)
+    Term last[2];
+};
+
+static_assert(sizeof(Plan) % 4 == 0, "plans are copied to shared memory word by word");
+
+struct AppDef {
+    int num_runs;          // sequential pattern runs (each re-scatters every v0)
+    Plan plans[6];
+    int num_counts;
+    uint32_t mult[6];
+    bool clique;           // counts k-cliques: eligible for the bitmap engine
+    int clique_k;
+};
+
+const AppDef &app_def(int app);
+
+// ---------------------------------------------------------------------------------
+// Device graph
+// ---------------------------------------------------------------------------------
+struct Graph {
+    uint32_t n = 0;
+    uint64_t m = 0;          // CSR entries
+    uint32_t max_degree = 0;
+    bool oriented = false;
+    uint64_t *off = nullptr; // device n+1
+    uint32_t *adj = nullptr; // device m + kAdjPad
+    khz_graph oriented_view = 0;  // cached orientation of a symmetric graph (owned)
+    uint64_t bytes = 0;
+};
+
+// DFS job (one (graph, plan) run inside a launch)
+struct DfsJob {
+    const uint64_t *off;
+    const uint32_t *adj;
+    uint32_t n;
+    uint32_t plan_idx;     // index into the launch's plan table
+    uint64_t unit_begin;   // first global unit of this job
+    uint64_t num_units;    // = CSR entries (one level-1 candidate per unit)
+    uint32_t out_base;     // counter row (KHZ_MAX_COUNTS + 2 uint64 per job)
+    uint32_t min_deg;      // skip start vertices whose degree is below this (handled elsewhere)
+};
+
+// Workspace: per-launch device scratch owned by a context
+struct Workspace {
+    uint32_t *slots = nullptr;   // dfs warps * kNumSlots * slot_cap
+    uint64_t slot_bytes = 0;
+    uint64_t *counters = nullptr;  // small device scratch: queue heads, stats
+    uint64_t counters_bytes = 0;
+    void *tmp = nullptr;          // cub temp / lists
+    uint64_t tmp_bytes = 0;
+    uint64_t *pinned = nullptr;   // host pinned mirror for results
+    uint64_t pinned_bytes = 0;
+};
+
+void set_error(const char *fmt, ...);
+khz_status cuda_fail(cudaError_t e, const char *what);
+
+#define KHZ_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t _e = (call);                                    \
+        if (_e != cudaSuccess) return ::khz::cuda_fail(_e, #call);  \
+    } while (0)
+
+// graph construction (graph.cu)
+khz_status build_csr_from_device_pairs(const uint32_t *d_pairs, uint64_t m, uint32_t n, bool validate,
+                                       Graph *g, cudaStream_t s);
+khz_status orient_graph(const Graph &in, Graph *out, cudaStream_t s);
+khz_status generate_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                         Graph *g, cudaStream_t s);
+void free_graph_memory(Graph *g);
+
+// engines
+constexpr int kPhases = 4;  // bitmap warp tier, mid block tier, large block tier, DFS
+struct LaunchStats {
+    uint32_t launches = 0;
+    // optional per-phase event pairs (recorded around each phase's kernel when non-null)
+    cudaEvent_t *ev_begin = nullptr;
+    cudaEvent_t *ev_end = nullptr;
+    bool used[kPhases] = {false, false, false, false};
+    uint32_t phase_launches[kPhases] = {0, 0, 0, 0};
+    uint64_t *d_phase_bytes = nullptr;  // device [kPhases], instrumented runs add per-phase bytes
+};
+// DFS engine: runs jobs; d_out rows of (KHZ_MAX_COUNTS + 2) uint64 must be zeroed by the caller.
+khz_status dfs_run(const DfsJob *h_jobs, int n_jobs, const Plan *h_plans, int n_plans, uint32_t slot_cap,
+                   bool stats, int warps_per_sm, int chunk, uint64_t *d_out, Workspace *ws, cudaStream_t s,
+                   LaunchStats *ls);
+// Bitmap clique engine on an oriented graph: adds count / NumExtensions-without-n-and-m / bytes into
+// d_out[0], d_out[6], d_out[7].  Vertices whose out-degree exceeds the block tier are returned in
+// *overflow (device list) for the DFS engine.
+khz_status bitmap_clique_run(const Graph &g, int k, bool stats, int warp_max, int block_warps,
+                             uint64_t *d_out, Workspace *ws, cudaStream_t s, LaunchStats *ls,
+                             uint32_t *n_overflow);
+uint32_t bitmap_block_max_degree();
+
+}  // namespace khz

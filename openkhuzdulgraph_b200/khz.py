@@ -1,0 +1,278 @@
+"""Python view of libkhz_b200.so (the engine's C ABI, include/khz.h).
+
+This is a thin ctypes binding for tests, the bench and Python callers; the engine and
+its host logic are native.  There is no CPU fallback: if the library is missing the
+import fails with an explicit error.
+
+The names follow the reference's application API (AmadeusChan/OpenKhuzdulGraph):
+apps are the kautomine / kgraphpi pattern programs, `count()` is the
+`count->clear(); app->run(); count->evaluate()` sequence of their main()
+(kautomine/triangle.cc:211-216), and graphs are the .dgraph CSR of graph_loader.h.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkhz_b200.so")
+
+APPS = {
+    "kautomine_triangle": 0, "kautomine_four_clique": 1, "kautomine_five_clique": 2,
+    "kautomine_three_motif": 3, "kgraphpi_triangle": 4, "kgraphpi_four_clique": 5,
+    "kgraphpi_five_clique": 6, "kgraphpi_three_motif": 7, "kgraphpi_four_cycle": 8,
+    "kgraphpi_house": 9, "kgraphpi_tailed_triangle": 10, "kautomine_four_motif": 11,
+}
+APP_NAMES = {v: k for k, v in APPS.items()}
+MAX_COUNTS = 6
+
+EDGES_ON_DEVICE = 0x1
+ORIENT = 0x2
+UNCHECKED = 0x4
+
+ENGINE_AUTO, ENGINE_DFS, ENGINE_BITMAP = 0, 1, 2
+
+SETOP = {"intersect": 0, "subtract": 1, "intersect_count": 2, "bounded_intersect": 3,
+         "bounded_subtract": 4, "trim": 5, "trim_lower_bound": 6}
+
+STATUS = {0: "KHZ_OK", 1: "KHZ_ERR_ARG", 2: "KHZ_ERR_OOM", 3: "KHZ_ERR_OVERFLOW", 4: "KHZ_ERR_TIMEOUT",
+          5: "KHZ_ERR_CUDA", 6: "KHZ_ERR_FORMAT", 7: "KHZ_ERR_BUSY", 8: "KHZ_ERR_NOT_FOUND"}
+
+# every entry point include/khz.h declares
+EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_get_config",
+           "khz_last_error_string", "khz_abi_version", "khz_graph_from_edges", "khz_graph_load_dgraph",
+           "khz_graph_orient", "khz_graph_generate_rmat", "khz_graph_info_get", "khz_graph_export_csr",
+           "khz_graph_write_dgraph", "khz_graph_free", "khz_count", "khz_count_async", "khz_app_num_counts",
+           "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch"]
+
+
+class KhzError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+class GraphInfo(ctypes.Structure):
+    _fields_ = [("num_vertices", ctypes.c_uint32), ("max_degree", ctypes.c_uint32),
+                ("num_entries", ctypes.c_uint64), ("oriented", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("d_offsets", ctypes.c_void_p), ("d_adj", ctypes.c_void_p), ("device_bytes", ctypes.c_uint64)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("num_extensions", ctypes.c_uint64), ("algo_bytes", ctypes.c_uint64),
+                ("kernel_ms", ctypes.c_double), ("engine", ctypes.c_uint32), ("launches", ctypes.c_uint32),
+                ("phase_ms", ctypes.c_double * 4), ("phase_bytes", ctypes.c_uint64 * 4),
+                ("phase_launches", ctypes.c_uint32 * 4)]
+
+    PHASES = ["bitmap_warp_tier", "bitmap_mid_block_tier", "bitmap_large_block_tier", "dfs"]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_[:5]}
+        d["phase_ms"] = list(self.phase_ms)
+        d["phase_bytes"] = list(self.phase_bytes)
+        d["phase_launches"] = list(self.phase_launches)
+        return d
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("engine", ctypes.c_int32), ("want_algo_bytes", ctypes.c_int32),
+                ("dfs_warps_per_sm", ctypes.c_int32), ("dfs_chunk", ctypes.c_int32),
+                ("bitmap_warp_max", ctypes.c_int32), ("bitmap_block_warps", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 10)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("graph", ctypes.c_uint32), ("app", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the engine.  Raises if the native library has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libkhz_b200.so not found at %s; build it with "
+                              "`python -m openkhuzdulgraph_b200.build`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        P, u32, u64, i32, vp = ctypes.POINTER, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p
+        sigs = {
+            "khz_ctx_create": (i32, [i32, P(vp)]),
+            "khz_ctx_destroy": (i32, [vp]),
+            "khz_ctx_set_config": (i32, [vp, P(Config)]),
+            "khz_ctx_get_config": (i32, [vp, P(Config)]),
+            "khz_last_error_string": (ctypes.c_char_p, []),
+            "khz_abi_version": (i32, []),
+            "khz_graph_from_edges": (i32, [vp, vp, u64, u32, u32, P(u32), vp]),
+            "khz_graph_load_dgraph": (i32, [vp, ctypes.c_char_p, u32, P(u32)]),
+            "khz_graph_orient": (i32, [vp, u32, P(u32), vp]),
+            "khz_graph_generate_rmat": (i32, [vp, i32, i32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                              u64, u32, P(u32), vp]),
+            "khz_graph_info_get": (i32, [vp, u32, P(GraphInfo)]),
+            "khz_graph_export_csr": (i32, [vp, u32, vp, vp]),
+            "khz_graph_write_dgraph": (i32, [vp, u32, ctypes.c_char_p, vp]),
+            "khz_graph_free": (i32, [vp, u32]),
+            "khz_count": (i32, [vp, u32, i32, P(u64), P(Stats), vp]),
+            "khz_count_async": (i32, [vp, u32, i32, vp, vp]),
+            "khz_app_num_counts": (i32, [i32]),
+            "khz_app_multiplicity": (i32, [i32, i32]),
+            "khz_count_batch": (i32, [vp, P(Job), i32, P(u64), P(u64), P(Stats), vp]),
+            "khz_set_op_batch": (i32, [i32, vp, vp, vp, vp, vp, vp, vp, u32, vp]),
+        }
+        for name, (res, args) in sigs.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise KhzError(status, lib().khz_last_error_string().decode(errors="replace"))
+
+
+def _app_id(app):
+    return APPS[app] if isinstance(app, str) else int(app)
+
+
+def num_counts(app):
+    return lib().khz_app_num_counts(_app_id(app))
+
+
+class Graph:
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.handle = handle
+
+    def info(self):
+        gi = GraphInfo()
+        _check(lib().khz_graph_info_get(self.ctx.ptr, self.handle, ctypes.byref(gi)))
+        return gi
+
+    @property
+    def num_vertices(self):
+        return self.info().num_vertices
+
+    @property
+    def num_entries(self):
+        return self.info().num_entries
+
+    def export_csr(self):
+        gi = self.info()
+        off = np.empty(gi.num_vertices + 1, dtype=np.uint64)
+        adj = np.empty(max(gi.num_entries, 1), dtype=np.uint32)
+        _check(lib().khz_graph_export_csr(self.ctx.ptr, self.handle, off.ctypes.data, adj.ctypes.data))
+        return off, adj[: gi.num_entries]
+
+    def orient(self, stream=None):
+        h = ctypes.c_uint32(0)
+        _check(lib().khz_graph_orient(self.ctx.ptr, self.handle, ctypes.byref(h), stream))
+        return Graph(self.ctx, h.value)
+
+    def write_dgraph(self, path, labels=None):
+        lab = None
+        if labels is not None:
+            labels = np.ascontiguousarray(labels, dtype=np.uint32)
+            lab = labels.ctypes.data
+        _check(lib().khz_graph_write_dgraph(self.ctx.ptr, self.handle, path.encode(), lab))
+
+    def free(self):
+        if self.handle:
+            _check(lib().khz_graph_free(self.ctx.ptr, self.handle))
+            self.handle = 0
+
+
+class Context:
+    """One engine context on one device: owns the graphs and all device scratch
+    (the reference's DistributedApplication + engines, distributed_application.h:12-60)."""
+
+    def __init__(self, device=0):
+        p = ctypes.c_void_p()
+        _check(lib().khz_ctx_create(device, ctypes.byref(p)))
+        self.ptr = p
+
+    def close(self):
+        if self.ptr:
+            lib().khz_ctx_destroy(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def config(self):
+        c = Config()
+        _check(lib().khz_ctx_get_config(self.ptr, ctypes.byref(c)))
+        return c
+
+    def set_config(self, **kw):
+        c = self.config()
+        for k, v in kw.items():
+            setattr(c, k, v)
+        _check(lib().khz_ctx_set_config(self.ptr, ctypes.byref(c)))
+
+    def graph_from_edges(self, pairs, n, orient=False, validate=True, stream=None):
+        """pairs: (m, 2) uint32 numpy array on the host, or a CUDA tensor (device pointer)."""
+        flags = (ORIENT if orient else 0) | (0 if validate else UNCHECKED)
+        if hasattr(pairs, "data_ptr"):  # torch tensor
+            assert pairs.dtype.itemsize == 4 and pairs.is_contiguous()
+            ptr, m = pairs.data_ptr(), pairs.numel() // 2
+            if pairs.is_cuda:
+                flags |= EDGES_ON_DEVICE
+        else:
+            pairs = np.ascontiguousarray(pairs, dtype=np.uint32).reshape(-1, 2)
+            ptr, m = pairs.ctypes.data, pairs.shape[0]
+        h = ctypes.c_uint32(0)
+        _check(lib().khz_graph_from_edges(self.ptr, ptr, m, n, flags, ctypes.byref(h), stream))
+        return Graph(self, h.value)
+
+    def load_dgraph(self, path, orient=False):
+        h = ctypes.c_uint32(0)
+        _check(lib().khz_graph_load_dgraph(self.ptr, path.encode(), ORIENT if orient else 0, ctypes.byref(h)))
+        return Graph(self, h.value)
+
+    def generate_rmat(self, scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=1, orient=False, stream=None):
+        h = ctypes.c_uint32(0)
+        _check(lib().khz_graph_generate_rmat(self.ptr, scale, edge_factor, a, b, c, seed,
+                                             ORIENT if orient else 0, ctypes.byref(h), stream))
+        return Graph(self, h.value)
+
+    def count(self, graph, app, stream=None):
+        """-> (counts list, Stats)"""
+        aid = _app_id(app)
+        counts = (ctypes.c_uint64 * MAX_COUNTS)()
+        st = Stats()
+        _check(lib().khz_count(self.ptr, graph.handle, aid, counts, ctypes.byref(st), stream))
+        return [int(counts[i]) for i in range(num_counts(aid))], st
+
+    def count_async(self, graph, app, d_out_ptr, stream=None):
+        _check(lib().khz_count_async(self.ptr, graph.handle, _app_id(app), d_out_ptr, stream))
+
+    def count_batch(self, jobs, stream=None):
+        """jobs: list of (Graph, app) -> (list of count lists, list of NumExtensions, Stats)"""
+        arr = (Job * len(jobs))()
+        for i, (g, app) in enumerate(jobs):
+            arr[i].graph = g.handle
+            arr[i].app = _app_id(app)
+        counts = (ctypes.c_uint64 * (MAX_COUNTS * len(jobs)))()
+        ext = (ctypes.c_uint64 * len(jobs))()
+        st = Stats()
+        _check(lib().khz_count_batch(self.ptr, arr, len(jobs), counts, ext, ctypes.byref(st), stream))
+        out = []
+        for i, (_, app) in enumerate(jobs):
+            nc = num_counts(app)
+            out.append([int(counts[i * MAX_COUNTS + c]) for c in range(nc)])
+        return out, [int(x) for x in ext], st
+
+
+def set_op_batch(op, a_off, a, b_off=None, b=None, bound=None, out=None, out_len=None, stream=None):
+    """VertexSet ops over device tensors (torch CUDA tensors: a_off/b_off int64, the rest int32)."""
+    def ptr(t):
+        return None if t is None else t.data_ptr()
+    n_pairs = a_off.numel() - 1
+    _check(lib().khz_set_op_batch(SETOP[op] if isinstance(op, str) else op, ptr(a_off), ptr(a), ptr(b_off), ptr(b),
+                                  ptr(bound), ptr(out), ptr(out_len), n_pairs, stream))

@@ -1,0 +1,237 @@
+"""Parity of the CUDA engine (through the C ABI) with the reference's outputs and the oracle.
+
+Counts and NumExtensions are integers: every comparison is exact.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import golden_graph
+import orc
+
+pytestmark = pytest.mark.gpu
+
+ALL_APPS = list(orc.APPS)
+CLIQUES = ["kautomine_triangle", "kautomine_four_clique", "kautomine_five_clique",
+           "kgraphpi_triangle", "kgraphpi_four_clique", "kgraphpi_five_clique"]
+
+
+@pytest.fixture(scope="module")
+def graphs(golden, khz_ctx):
+    out = []
+    for spec in golden["graphs"]:
+        canon, n, sym, off, adj = golden_graph(spec)
+        g = khz_ctx.graph_from_edges(sym, n)
+        out.append((spec, n, sym, off, adj, g))
+    return out
+
+
+def test_csr_build_matches_oracle(graphs):
+    for spec, n, sym, off, adj, g in graphs:
+        goff, gadj = g.export_csr()
+        assert np.array_equal(goff, off), spec["name"]
+        assert np.array_equal(gadj, adj), spec["name"]
+        assert g.info().max_degree == int(np.diff(off).max())
+
+
+def test_orientation_matches_oracle(graphs, khz_ctx):
+    for spec, n, sym, off, adj, g in graphs:
+        og = g.orient()
+        ooff, oadj, _ = orc.orient(off, adj)
+        goff, gadj = og.export_csr()
+        assert np.array_equal(goff, ooff), spec["name"]
+        assert np.array_equal(gadj, oadj), spec["name"]
+        og.free()
+
+
+def test_write_dgraph_matches_reference_bytes(graphs, khz_ctx):
+    import hashlib
+    with tempfile.TemporaryDirectory() as td:
+        for spec, n, sym, off, adj, g in graphs:
+            p = os.path.join(td, "g.dgraph")
+            g.write_dgraph(p)
+            with open(p, "rb") as f:
+                assert hashlib.sha256(f.read()).hexdigest() == spec["sha256_dgraph"], spec["name"]
+            if spec["sha256_oriented"]:
+                og = g.orient()
+                og.write_dgraph(p)
+                with open(p, "rb") as f:
+                    assert hashlib.sha256(f.read()).hexdigest() == spec["sha256_oriented"], spec["name"]
+                og.free()
+
+
+def test_load_dgraph(graphs, khz_ctx):
+    with tempfile.TemporaryDirectory() as td:
+        spec, n, sym, off, adj, _ = graphs[2]
+        p = os.path.join(td, "g.dgraph")
+        orc.write_dgraph(p, n, sym, labels=np.arange(n, dtype=np.uint32) % 3)
+        g = khz_ctx.load_dgraph(p)
+        goff, gadj = g.export_csr()
+        assert np.array_equal(goff, off) and np.array_equal(gadj, adj)
+        g.free()
+
+
+@pytest.mark.parametrize("engine", ["auto", "dfs"])
+@pytest.mark.parametrize("app", ALL_APPS)
+def test_counts_match_reference(graphs, golden, khz_ctx, app, engine):
+    """Symmetric input: counts and NumExtensions equal the reference apps' (golden) or the oracle's."""
+    from openkhuzdulgraph_b200 import khz
+    khz_ctx.set_config(engine=khz.ENGINE_AUTO if engine == "auto" else khz.ENGINE_DFS, want_algo_bytes=0)
+    for spec, n, sym, off, adj, g in graphs:
+        counts, st = khz_ctx.count(g, app)
+        ref = spec["apps"].get(app)
+        if ref is not None:
+            assert counts == ref["counts"], (spec["name"], app)
+            assert st.num_extensions == ref["num_extensions"], (spec["name"], app)
+        else:
+            oc, oext, _ = orc.count(app, off, adj)
+            assert counts == oc, (spec["name"], app)
+            assert st.num_extensions == oext, (spec["name"], app)
+    khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+
+
+@pytest.mark.parametrize("app", ALL_APPS)
+def test_algorithmic_bytes_match_oracle(graphs, khz_ctx, app):
+    """The instrumented DFS variant sums the same set-op sizes as the restated schedule."""
+    from openkhuzdulgraph_b200 import khz
+    khz_ctx.set_config(engine=khz.ENGINE_DFS, want_algo_bytes=1)
+    try:
+        for spec, n, sym, off, adj, g in graphs[:5]:
+            counts, st = khz_ctx.count(g, app)
+            oc, oext, obytes = orc.count(app, off, adj)
+            assert counts == oc and st.num_extensions == oext
+            assert st.algo_bytes == obytes, (spec["name"], app)
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO, want_algo_bytes=0)
+
+
+@pytest.mark.parametrize("engine", ["bitmap", "dfs"])
+@pytest.mark.parametrize("app", CLIQUES)
+def test_cliques_on_oriented_input(graphs, golden, khz_ctx, app, engine):
+    from openkhuzdulgraph_b200 import khz
+    khz_ctx.set_config(engine=khz.ENGINE_BITMAP if engine == "bitmap" else khz.ENGINE_DFS, want_algo_bytes=1)
+    try:
+        for spec, n, sym, off, adj, g in graphs:
+            og = khz_ctx.graph_from_edges(sym, n, orient=True)
+            counts, st = khz_ctx.count(og, app)
+            ooff, oadj, _ = orc.orient(off, adj)
+            oc, oext, obytes = orc.count(app, ooff, oadj)
+            ref = spec["apps_oriented"].get(app)
+            if ref is not None:
+                assert oc == ref["counts"] and oext == ref["num_extensions"]
+            assert counts == oc, (spec["name"], app, engine)
+            assert st.num_extensions == oext, (spec["name"], app, engine)
+            assert st.algo_bytes == obytes, (spec["name"], app, engine)
+            og.free()
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO, want_algo_bytes=0)
+
+
+def test_rmat_generator_matches_oracle(khz_ctx):
+    for scale, ef, seed in [(8, 4, 1), (10, 8, 3), (12, 16, 2)]:
+        canon, n = orc.rmat(scale, ef, seed=seed)
+        off, adj = orc.csr(orc.symmetrize(canon), n)
+        g = khz_ctx.generate_rmat(scale, ef, seed=seed)
+        goff, gadj = g.export_csr()
+        assert np.array_equal(goff, off) and np.array_equal(gadj, adj), (scale, ef, seed)
+        g.free()
+
+
+def test_invalid_inputs_are_rejected(khz_ctx):
+    from openkhuzdulgraph_b200 import khz
+    bad_sets = [
+        np.array([[1, 0], [0, 1]], dtype=np.uint32),   # unsorted
+        np.array([[0, 1], [0, 1]], dtype=np.uint32),   # duplicate
+        np.array([[0, 0]], dtype=np.uint32),           # self-loop
+        np.array([[0, 5]], dtype=np.uint32),           # id >= n
+    ]
+    for pairs in bad_sets:
+        with pytest.raises(khz.KhzError) as e:
+            khz_ctx.graph_from_edges(pairs, 3)
+        assert e.value.status == 6
+    g = khz_ctx.graph_from_edges(np.array([[0, 1], [1, 0]], dtype=np.uint32), 2)
+    with pytest.raises(khz.KhzError) as e:
+        khz_ctx.count(g, 77)
+    assert e.value.status == 1
+    g.free()
+    with pytest.raises(khz.KhzError):
+        khz_ctx.count(g, 0)
+    # empty graph and isolated vertices
+    e0 = khz_ctx.graph_from_edges(np.zeros((0, 2), dtype=np.uint32), 5)
+    for app in ALL_APPS:
+        counts, st = khz_ctx.count(e0, app)
+        assert all(c == 0 for c in counts) and st.num_extensions == 5 * {7: 2, 11: 6}.get(orc.APPS[app], 1)
+    e0.free()
+
+
+def test_set_op_batch_matches_oracle(khz_ctx):
+    import torch
+    from openkhuzdulgraph_b200 import khz
+    rng = np.random.default_rng(1)
+    lists_a, lists_b = [[], [1, 2, 3], [], [5], [0, 2**32 - 1]], [[], [], [4, 5], [5], [2**32 - 1]]
+    for _ in range(300):
+        sa = int(rng.choice([0, 3, 40, 300, 2000]))
+        sb = int(rng.choice([0, 5, 50, 700, 5000]))
+        lists_a.append(np.unique(rng.integers(0, 6000, sa)).tolist())
+        lists_b.append(np.unique(rng.integers(0, 6000, sb)).tolist())
+    a_off = np.cumsum([0] + [len(x) for x in lists_a]).astype(np.int64)
+    b_off = np.cumsum([0] + [len(x) for x in lists_b]).astype(np.int64)
+    a = np.array(sum(lists_a, []) + [0], dtype=np.uint32)
+    b = np.array(sum(lists_b, []) + [0], dtype=np.uint32)
+    bounds = rng.integers(0, 6000, len(lists_a)).astype(np.uint32)
+    dev = "cuda"
+    ta_off, tb_off = torch.from_numpy(a_off).to(dev), torch.from_numpy(b_off).to(dev)
+    ta, tb = torch.from_numpy(a.view(np.int32)).to(dev), torch.from_numpy(b.view(np.int32)).to(dev)
+    tbound = torch.from_numpy(bounds.view(np.int32)).to(dev)
+    L = orc.lib()
+    for op in ["intersect", "subtract", "intersect_count", "bounded_intersect", "bounded_subtract", "trim",
+               "trim_lower_bound"]:
+        out = torch.zeros(max(len(a), 1), dtype=torch.int32, device=dev)
+        out_len = torch.zeros(len(lists_a), dtype=torch.int32, device=dev)
+        khz.set_op_batch(op, ta_off, ta, tb_off, tb, tbound, out, out_len)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy().view(np.uint32)
+        glen = out_len.cpu().numpy().view(np.uint32)
+        for i, (la, lb) in enumerate(zip(lists_a, lists_b)):
+            A = np.array(la + [0], dtype=np.uint32)
+            B = np.array(lb + [0], dtype=np.uint32)
+            buf = np.zeros(len(la) + 1, dtype=np.uint32)
+            ub = int(bounds[i])
+            if op == "intersect":
+                r = L.orc_intersect(A, len(la), B, len(lb), buf)
+            elif op == "subtract":
+                r = L.orc_subtract(A, len(la), B, len(lb), buf)
+            elif op == "intersect_count":
+                r = L.orc_intersect_count(A, len(la), B, len(lb))
+            elif op == "bounded_intersect":
+                r = L.orc_bounded_intersect(A, len(la), B, len(lb), ub, buf)
+            elif op == "bounded_subtract":
+                r = L.orc_bounded_subtract(A, len(la), B, len(lb), ub, buf)
+            elif op == "trim":
+                r = L.orc_trim(A, len(la), ub)
+            else:
+                r = L.orc_trim_lower_bound(A, len(la), ub)
+            assert glen[i] == r, (op, i)
+            if op in ("intersect", "subtract", "bounded_intersect", "bounded_subtract"):
+                s = int(a_off[i])
+                assert got[s:s + r].tolist() == buf[:r].tolist(), (op, i)
+
+
+def test_batch_matches_single(graphs, khz_ctx):
+    jobs = []
+    for spec, n, sym, off, adj, g in graphs:
+        for app in ["kautomine_triangle", "kautomine_four_clique", "kgraphpi_four_cycle", "kautomine_three_motif"]:
+            jobs.append((g, app))
+    counts, exts, st = khz_ctx.count_batch(jobs)
+    for (g, app), c, e in zip(jobs, counts, exts):
+        c1, st1 = khz_ctx.count(g, app)
+        assert c == c1 and e == st1.num_extensions, app
+
+
+def test_deterministic_repeat(graphs, khz_ctx):
+    g = graphs[3][5]
+    a = [khz_ctx.count(g, app)[0] for app in ALL_APPS]
+    b = [khz_ctx.count(g, app)[0] for app in ALL_APPS]
+    assert a == b
