@@ -72,8 +72,8 @@ typedef struct khz_graph_info {
     uint32_t num_vertices;
     uint32_t max_degree;
     uint64_t num_entries;  /* CSR entries: 2|E| symmetric, |E| oriented */
-    int32_t oriented;
-    int32_t reserved;
+    int32_t oriented;      /* 1: every list holds only larger ids (a DAG in id order) */
+    int32_t symmetric;     /* 1: every entry has its reverse (undirected form) */
     const uint64_t *d_offsets; /* device, num_vertices + 1 */
     const uint32_t *d_adj;     /* device, num_entries (+ 4 padding entries) */
     uint64_t device_bytes;     /* HBM held by this graph */

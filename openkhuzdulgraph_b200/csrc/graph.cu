@@ -33,6 +33,31 @@ __global__ void validate_pairs_kernel(const uint32_t *__restrict__ pairs, uint64
             ok = ok && ck > pk;
         }
         if (!ok) atomicOr(bad, 1u);
+        if (s >= d) atomicOr(bad + 1, 1u);  // not upper-triangular
+    }
+}
+
+// every entry (u, v) must have its reverse (v, u): one binary search per entry
+__global__ void symmetry_kernel(const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t n,
+                                unsigned int *asym) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t u = warp; u < n; u += nwarps) {
+        const uint64_t b = off[u], e = off[u + 1];
+        bool bad = false;
+        for (uint64_t i = b + lane; i < e; i += 32) {
+            const uint32_t v = adj[i];
+            uint64_t l = off[v], r = off[v + 1];
+            while (l < r) {
+                const uint64_t mid = (l + r) >> 1;
+                if (adj[mid] < u) l = mid + 1; else r = mid;
+            }
+            bad = bad || !(l < off[v + 1] && adj[l] == u);
+        }
+        if (__any_sync(0xffffffffu, bad)) {
+            if (lane == 0) atomicOr(asym, 1u);
+        }
     }
 }
 
@@ -192,18 +217,21 @@ khz_status build_csr_from_device_pairs(const uint32_t *d_pairs, uint64_t m, uint
         return KHZ_ERR_FORMAT;
     }
     DevBuf flag;
+    KHZ_CUDA(cudaMalloc(&flag.p, sizeof(unsigned int) * 4));
+    KHZ_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(unsigned int) * 4, s));
+    unsigned int hflags[4] = {0, 1, 1, 0};  // bad, not_upper, asym (unknown without validation)
     if (validate && m > 0) {
-        KHZ_CUDA(cudaMalloc(&flag.p, sizeof(unsigned int) * 2));
-        KHZ_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(unsigned int) * 2, s));
         validate_pairs_kernel<<<grid_for(m, sms), 256, 0, s>>>(d_pairs, m, n, (unsigned int *)flag.p);
         KHZ_CUDA(cudaGetLastError());
-        unsigned int bad = 0;
-        KHZ_CUDA(cudaMemcpyAsync(&bad, flag.p, sizeof(bad), cudaMemcpyDeviceToHost, s));
+        KHZ_CUDA(cudaMemcpyAsync(hflags, flag.p, sizeof(unsigned int) * 2, cudaMemcpyDeviceToHost, s));
         KHZ_CUDA(cudaStreamSynchronize(s));
-        if (bad) {
+        if (hflags[0]) {
             set_error("edge list is not sorted by (src, dst), has duplicates or self-loops, or ids >= n");
             return KHZ_ERR_FORMAT;
         }
+    } else if (validate) {
+        hflags[1] = 0;  // an empty graph is both upper-triangular and symmetric
+        hflags[2] = 0;
     }
     Graph out;
     out.n = n;
@@ -218,10 +246,15 @@ khz_status build_csr_from_device_pairs(const uint32_t *d_pairs, uint64_t m, uint
     cudaMemsetAsync(out.adj + m, 0xff, kAdjPad * sizeof(uint32_t), s);
     boundaries_kernel<<<grid_for(m + 1, sms), 256, 0, s>>>(d_pairs, m, n, out.off);
     if (m > 0) extract_dst_kernel<<<grid_for(m, sms), 256, 0, s>>>(d_pairs, m, out.adj);
-    unsigned int *d_max = nullptr;
-    if (!flag.p) KHZ_CUDA(cudaMalloc(&flag.p, sizeof(unsigned int) * 2));
-    d_max = (unsigned int *)flag.p + 1;
+    unsigned int *d_max = (unsigned int *)flag.p + 3;
     KHZ_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned int), s));
+    if (validate && m > 0 && hflags[1]) {
+        // not a DAG in id order: find out whether it is the symmetric (undirected) form
+        symmetry_kernel<<<grid_for((uint64_t)n * 32, sms), 256, 0, s>>>(out.off, out.adj, n,
+                                                                         (unsigned int *)flag.p + 2);
+        KHZ_CUDA(cudaMemcpyAsync(&hflags[2], (unsigned int *)flag.p + 2, sizeof(unsigned int),
+                                 cudaMemcpyDeviceToHost, s));
+    }
     if (n > 0) max_degree_kernel<<<grid_for(n, sms), 256, 0, s>>>(out.off, n, d_max);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -232,6 +265,8 @@ khz_status build_csr_from_device_pairs(const uint32_t *d_pairs, uint64_t m, uint
     KHZ_CUDA(cudaMemcpyAsync(&mx, d_max, sizeof(mx), cudaMemcpyDeviceToHost, s));
     KHZ_CUDA(cudaStreamSynchronize(s));
     out.max_degree = mx;
+    out.oriented = hflags[1] == 0;
+    out.symmetric = hflags[2] == 0;
     out.bytes = ((uint64_t)n + 1) * 8 + (m + kAdjPad) * 4;
     *g = out;
     return KHZ_OK;
@@ -309,6 +344,8 @@ khz_status orient_graph(const Graph &in, Graph *outg, cudaStream_t s) {
         return cuda_fail(e, "orientation");
     }
     out.max_degree = mx;
+    out.oriented = true;
+    out.symmetric = out.m == 0;
     out.bytes = ((uint64_t)n + 1) * 8 + (out.m + kAdjPad) * 4;
     *outg = out;
     return KHZ_OK;
@@ -389,7 +426,12 @@ khz_status generate_rmat(int scale, int edge_factor, double a, double b, double 
                                                 (int64_t)(2 * m), 0, 64, s));
     if (m > 0) keys_to_pairs_kernel<<<grid_for(2 * m, sms), 256, 0, s>>>((uint64_t *)sym_sorted.p, 2 * m);
     KHZ_CUDA(cudaGetLastError());
-    return build_csr_from_device_pairs((const uint32_t *)sym_sorted.p, 2 * m, n, false, g, s);
+    khz_status st = build_csr_from_device_pairs((const uint32_t *)sym_sorted.p, 2 * m, n, false, g, s);
+    if (st == KHZ_OK) {
+        g->symmetric = true;  // both directions of every edge by construction
+        g->oriented = m == 0;
+    }
+    return st;
 }
 
 }  // namespace khz

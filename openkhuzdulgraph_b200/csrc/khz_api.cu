@@ -204,6 +204,9 @@ khz_status enqueue_count(khz_ctx *ctx, khz_graph h, int app, size_t row, std::ve
     if (engine == KHZ_ENGINE_AUTO) engine = def.clique ? KHZ_ENGINE_BITMAP : KHZ_ENGINE_DFS;
     if (engine == KHZ_ENGINE_BITMAP && !def.clique) engine = KHZ_ENGINE_DFS;
     uint64_t *raw = ctx->d_rows + row * kRow;
+    // the bitmap engine needs a DAG in id order; a symmetric graph is oriented first (cached);
+    // any other shape runs the schedule as stored, like the reference does
+    if (engine == KHZ_ENGINE_BITMAP && !g->oriented && !g->symmetric) engine = KHZ_ENGINE_DFS;
     if (engine == KHZ_ENGINE_BITMAP && !batched) {
         Graph *og = nullptr;
         khz_status st = oriented_of(ctx, h, &og, s);
@@ -303,7 +306,9 @@ khz_status count_many(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64_t *d
     if (!batched) {
         const AppDef &def = app_def(jobs[0].app);
         int engine = ctx->cfg.engine;
-        if ((engine == KHZ_ENGINE_AUTO || engine == KHZ_ENGINE_BITMAP) && def.clique) {
+        Graph *g0 = get_graph(ctx, jobs[0].graph);
+        if ((engine == KHZ_ENGINE_AUTO || engine == KHZ_ENGINE_BITMAP) && def.clique && !g0->oriented &&
+            g0->symmetric) {
             Graph *og;
             st = oriented_of(ctx, jobs[0].graph, &og, s);
             if (st) return st;
@@ -594,6 +599,7 @@ khz_status khz_graph_info_get(khz_ctx *ctx, khz_graph h, khz_graph_info *info) {
     info->num_entries = g->m;
     info->max_degree = g->max_degree;
     info->oriented = g->oriented ? 1 : 0;
+    info->symmetric = g->symmetric ? 1 : 0;
     info->d_offsets = g->off;
     info->d_adj = g->adj;
     info->device_bytes = g->bytes;

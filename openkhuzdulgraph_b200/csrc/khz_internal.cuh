@@ -75,7 +75,8 @@ struct Graph {
     uint32_t n = 0;
     uint64_t m = 0;          // CSR entries
     uint32_t max_degree = 0;
-    bool oriented = false;
+    bool oriented = false;   // every list holds only ids above its vertex (a DAG in id order)
+    bool symmetric = false;  // every entry (u, v) has its reverse (v, u)
     uint64_t *off = nullptr; // device n+1
     uint32_t *adj = nullptr; // device m + kAdjPad
     khz_graph oriented_view = 0;  // cached orientation of a symmetric graph (owned)

@@ -54,7 +54,7 @@ class KhzError(RuntimeError):
 
 class GraphInfo(ctypes.Structure):
     _fields_ = [("num_vertices", ctypes.c_uint32), ("max_degree", ctypes.c_uint32),
-                ("num_entries", ctypes.c_uint64), ("oriented", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("num_entries", ctypes.c_uint64), ("oriented", ctypes.c_int32), ("symmetric", ctypes.c_int32),
                 ("d_offsets", ctypes.c_void_p), ("d_adj", ctypes.c_void_p), ("device_bytes", ctypes.c_uint64)]
 
 

@@ -235,3 +235,31 @@ def test_deterministic_repeat(graphs, khz_ctx):
     a = [khz_ctx.count(g, app)[0] for app in ALL_APPS]
     b = [khz_ctx.count(g, app)[0] for app in ALL_APPS]
     assert a == b
+
+
+def test_graph_shape_detection_and_as_stored_semantics(graphs, khz_ctx):
+    """An oriented edge list is counted as stored (bitmap engine); a directed graph that is
+    neither symmetric nor a DAG runs the schedule as stored, like the reference does."""
+    spec, n, sym, off, adj, g = graphs[3]
+    gi = g.info()
+    assert gi.symmetric == 1 and gi.oriented == 0
+    ooff, oadj, _ = orc.orient(off, adj)
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(ooff).astype(np.int64))
+    og = khz_ctx.graph_from_edges(np.stack([src, oadj], axis=1), n)
+    oi = og.info()
+    assert oi.oriented == 1 and oi.symmetric == 0
+    for app in CLIQUES:
+        assert khz_ctx.count(og, app)[0] == orc.count(app, ooff, oadj)[0], app
+    og.free()
+    # a directed graph: keep (u, v) when (u + v) is even or u < v
+    keep = ((sym[:, 0] + sym[:, 1]) % 2 == 0) | (sym[:, 0] < sym[:, 1])
+    dpairs = np.ascontiguousarray(sym[keep])
+    doff, dadj = orc.csr(dpairs, n)
+    dg = khz_ctx.graph_from_edges(dpairs, n)
+    di = dg.info()
+    assert di.oriented == 0 and di.symmetric == 0
+    for app in ALL_APPS:
+        got, st = khz_ctx.count(dg, app)
+        exp, ext, _ = orc.count(app, doff, dadj)
+        assert got == exp and st.num_extensions == ext, app
+    dg.free()
