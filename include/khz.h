@@ -32,7 +32,10 @@ typedef enum khz_status {
     KHZ_ERR_CUDA = 5,     /* a CUDA runtime call failed */
     KHZ_ERR_FORMAT = 6,   /* input graph violates the .dgraph contract */
     KHZ_ERR_BUSY = 7,     /* serving queue full / ticket not finished */
-    KHZ_ERR_NOT_FOUND = 8
+    KHZ_ERR_NOT_FOUND = 8,
+    KHZ_ERR_MULTIPLICITY = 9 /* a raw count is not divisible by the pattern multiplicity: the input
+                                is not the undirected graph the app assumes (the reference asserts,
+                                kautomine/three_motif.cc:232,243) */
 } khz_status;
 
 /* Pattern applications; the numbering is shared with the oracle.

@@ -728,8 +728,8 @@ khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts
     KHZ_CUDA(cudaMemcpyAsync(&bad, ctx->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
     KHZ_CUDA(cudaStreamSynchronize(s));
     if (bad) {
-        set_error("raw count not divisible by the pattern multiplicity");
-        return KHZ_ERR_OVERFLOW;
+        set_error("raw count not divisible by the pattern multiplicity (input is not an undirected graph)");
+        return KHZ_ERR_MULTIPLICITY;
     }
     const int nc = app_def(app).num_counts;
     for (int c = 0; c < nc; ++c) counts[c] = row[c];
@@ -768,8 +768,8 @@ khz_status khz_count_batch(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64
     KHZ_CUDA(cudaMemcpyAsync(&bad, ctx->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
     KHZ_CUDA(cudaStreamSynchronize(s));
     if (bad) {
-        set_error("raw count not divisible by the pattern multiplicity");
-        return KHZ_ERR_OVERFLOW;
+        set_error("raw count not divisible by the pattern multiplicity (input is not an undirected graph)");
+        return KHZ_ERR_MULTIPLICITY;
     }
     for (int i = 0; i < n_jobs; ++i) {
         for (int c = 0; c < KHZ_MAX_COUNTS; ++c) counts[(size_t)i * KHZ_MAX_COUNTS + c] = rows[(size_t)i * kRow + c];

@@ -36,7 +36,8 @@ SETOP = {"intersect": 0, "subtract": 1, "intersect_count": 2, "bounded_intersect
          "bounded_subtract": 4, "trim": 5, "trim_lower_bound": 6}
 
 STATUS = {0: "KHZ_OK", 1: "KHZ_ERR_ARG", 2: "KHZ_ERR_OOM", 3: "KHZ_ERR_OVERFLOW", 4: "KHZ_ERR_TIMEOUT",
-          5: "KHZ_ERR_CUDA", 6: "KHZ_ERR_FORMAT", 7: "KHZ_ERR_BUSY", 8: "KHZ_ERR_NOT_FOUND"}
+          5: "KHZ_ERR_CUDA", 6: "KHZ_ERR_FORMAT", 7: "KHZ_ERR_BUSY", 8: "KHZ_ERR_NOT_FOUND",
+          9: "KHZ_ERR_MULTIPLICITY"}
 
 # every entry point include/khz.h declares
 EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_get_config",

@@ -258,8 +258,16 @@ def test_graph_shape_detection_and_as_stored_semantics(graphs, khz_ctx):
     dg = khz_ctx.graph_from_edges(dpairs, n)
     di = dg.info()
     assert di.oriented == 0 and di.symmetric == 0
+    from openkhuzdulgraph_b200 import khz
     for app in ALL_APPS:
+        try:
+            exp, ext, _ = orc.count(app, doff, dadj)
+        except RuntimeError:
+            # the raw count is not divisible by the multiplicity: the reference asserts here
+            with pytest.raises(khz.KhzError) as e:
+                khz_ctx.count(dg, app)
+            assert e.value.status == 9, app
+            continue
         got, st = khz_ctx.count(dg, app)
-        exp, ext, _ = orc.count(app, doff, dadj)
         assert got == exp and st.num_extensions == ext, app
     dg.free()
