@@ -183,6 +183,22 @@ khz_status khz_set_op_batch(int op, const uint64_t *a_off, const uint32_t *a, co
                             const uint32_t *b, const uint32_t *bound, uint32_t *out, uint32_t *out_len,
                             uint32_t n_pairs, void *stream);
 
+/* ---- counting without device allocation ------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc: host frameworks
+ * that own all device memory through their own pool and forbid side allocations, or plugins
+ * loaded into a process whose allocator is locked down.  Counts `app` on a caller-owned device
+ * CSR (d_offsets: n + 1 uint64, d_adj: num_entries uint32) with the DFS engine and writes the
+ * same 8 uint64 as khz_count_async to the caller's device buffer d_out: [0..5] counts,
+ * [6] NumExtensions, [7] 0.  It allocates nothing: all scratch lives in one fixed device array
+ * of about 14.6 MiB inside the library, which every GPU that loads the library holds until the
+ * process exits.  Limits: graphs whose largest vertex degree is at most 1024 (larger ones get
+ * KHZ_ERR_ARG).  The first call on each device looks up the array's device address with that
+ * device current, so make that first call before any stream capture.  Every call shares the
+ * array: calls whose work overlaps on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller.  Returns once d_out holds the result. */
+khz_status khz_count_noalloc(const uint64_t *d_offsets, const uint32_t *d_adj, uint32_t n, uint64_t num_entries,
+                             khz_app_id app, uint64_t *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

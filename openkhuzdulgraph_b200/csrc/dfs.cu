@@ -277,6 +277,17 @@ __global__ void __launch_bounds__(256) dfs_kernel(const DfsJob *__restrict__ job
 
 }  // namespace
 
+// Launch the (uninstrumented) DFS kernel on caller-provided device tables and scratch; no
+// allocation and no host synchronisation.
+khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_plans, uint64_t total_units,
+                               uint32_t chunk, uint32_t *slots, uint32_t slot_cap, unsigned long long *queue,
+                               uint64_t *d_raw, int blocks, int threads, cudaStream_t s) {
+    dfs_kernel<false><<<blocks, threads, 0, s>>>(d_jobs, n_jobs, d_plans, total_units, chunk, slots, slot_cap, queue,
+                                                 d_raw, nullptr);
+    KHZ_CUDA(cudaGetLastError());
+    return KHZ_OK;
+}
+
 khz_status dfs_run(const DfsJob *h_jobs, int n_jobs, const Plan *h_plans, int n_plans, uint32_t slot_cap,
                    bool stats, int warps_per_sm, int chunk, uint64_t *d_out, Workspace *ws, cudaStream_t s,
                    LaunchStats *ls) {

@@ -139,6 +139,9 @@ struct LaunchStats {
 khz_status dfs_run(const DfsJob *h_jobs, int n_jobs, const Plan *h_plans, int n_plans, uint32_t slot_cap,
                    bool stats, int warps_per_sm, int chunk, uint64_t *d_out, Workspace *ws, cudaStream_t s,
                    LaunchStats *ls);
+khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_plans, uint64_t total_units,
+                               uint32_t chunk, uint32_t *slots, uint32_t slot_cap, unsigned long long *queue,
+                               uint64_t *d_raw, int blocks, int threads, cudaStream_t s);
 // Bitmap clique engine on an oriented graph: adds count / NumExtensions-without-n-and-m / bytes into
 // d_out[0], d_out[6], d_out[7].  Vertices whose out-degree exceeds the block tier are returned in
 // *overflow (device list) for the DFS engine.

@@ -44,7 +44,7 @@ EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_g
            "khz_last_error_string", "khz_abi_version", "khz_graph_from_edges", "khz_graph_load_dgraph",
            "khz_graph_orient", "khz_graph_generate_rmat", "khz_graph_info_get", "khz_graph_export_csr",
            "khz_graph_write_dgraph", "khz_graph_free", "khz_count", "khz_count_async", "khz_app_num_counts",
-           "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch"]
+           "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch", "khz_count_noalloc"]
 
 
 class KhzError(RuntimeError):
@@ -120,6 +120,7 @@ def lib():
             "khz_app_multiplicity": (i32, [i32, i32]),
             "khz_count_batch": (i32, [vp, P(Job), i32, P(u64), P(u64), P(Stats), vp]),
             "khz_set_op_batch": (i32, [i32, vp, vp, vp, vp, vp, vp, vp, u32, vp]),
+            "khz_count_noalloc": (i32, [vp, vp, u32, u64, i32, vp, vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -268,6 +269,13 @@ class Context:
             nc = num_counts(app)
             out.append([int(counts[i * MAX_COUNTS + c]) for c in range(nc)])
         return out, [int(x) for x in ext], st
+
+
+def count_noalloc(d_offsets, d_adj, n, num_entries, app, d_out, stream=None):
+    """Count through the entry point that allocates no device memory (for callers whose
+    device memory is owned by a pool they may not bypass).  All pointers are device pointers
+    (ints); d_out receives 8 uint64.  Degree limit 1024; overlapping calls race."""
+    _check(lib().khz_count_noalloc(d_offsets, d_adj, n, num_entries, _app_id(app), d_out, stream))
 
 
 def set_op_batch(op, a_off, a, b_off=None, b=None, bound=None, out=None, out_len=None, stream=None):
