@@ -30,7 +30,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-SCALE, EDGE_FACTOR, SEED = 22, 16, 1
+SCALE, EDGE_FACTOR, SEED = 22, 16, 1   # defaults; --scale / --edge-factor select a smaller case for profiling
 RMAT_ABC = (0.57, 0.19, 0.19)
 APP = "kautomine_four_clique"
 SAMPLE_MOD = 32      # CPU sample: start vertices with v0 % 32 == 0 (one label class of 32)
@@ -174,7 +174,7 @@ def ours(args, rank, world, local):
     dev = torch.device("cuda", local)
     ctx = khz.Context(local)
     a, b, c = RMAT_ABC
-    sym = ctx.generate_rmat(SCALE, EDGE_FACTOR, a, b, c, SEED)
+    sym = ctx.generate_rmat(args.scale, args.edge_factor, a, b, c, SEED)
     g = sym.orient()
     gi = g.info()
     n, m = gi.num_vertices, gi.num_entries
@@ -222,6 +222,14 @@ def ours(args, rank, world, local):
             traffic = json.load(f).get(khz.Stats.PHASES[dom])
 
     # e2e: oriented .dgraph edge list in pinned host memory -> C ABI -> count -> host
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "embeddings/s", "ms_per_step": ms_per_step,
+                              "phase_ms_per_step": [x / args.steps for x in phase_ms],
+                              "phase_algo_bytes": list(st_stats.phase_bytes), "count": ref_counts[0],
+                              "scale": args.scale, "edge_factor": args.edge_factor}), flush=True)
+        ctx.close()
+        return
     off_h, adj_h = g.export_csr()
     src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off_h).astype(np.int64))
     pairs = torch.from_numpy(np.stack([src, adj_h], axis=1).reshape(-1).view(np.int32)).pin_memory()
@@ -284,7 +292,7 @@ def reference_arm(args, rank, world, local):
     torch.cuda.set_device(local)
     ctx = khz.Context(local)
     a, b, c = RMAT_ABC
-    sym = ctx.generate_rmat(SCALE, EDGE_FACTOR, a, b, c, SEED)
+    sym = ctx.generate_rmat(args.scale, args.edge_factor, a, b, c, SEED)
     g = sym.orient()
     sym.free()
     with tempfile.TemporaryDirectory() as td:
@@ -309,6 +317,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="device-resident steps only (profiling)")
+    ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the bench workload is 22)")
+    ap.add_argument("--edge-factor", type=int, default=EDGE_FACTOR, help="R-MAT edge factor (workload: 16)")
     args = ap.parse_args()
     if args.impl == "reference":
         # the reference arm is a CPU run on rank 0; other ranks exit without work
