@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kWarpMax = 64;          // warp tier: d <= 64 -> 2 words per row
 constexpr int kMidMax = 256;          // mid block tier
-constexpr int kBlockMax = 1248;       // large block tier: 1248 rows x 39 words = 190 KiB
+constexpr int kBlockMax = 1216;       // large block tier: 1216 rows x 38 words = 180 KiB (+ hash 24 KiB)
 
 // position of the n-th (0-based) set bit of x; x must have more than n set bits
 __device__ __forceinline__ int nth_set_bit(uint32_t x, int n) {
@@ -58,63 +58,116 @@ __device__ __forceinline__ uint32_t odeg(const uint64_t *off, uint32_t v) {
     return (uint32_t)(__ldg(off + v + 1) - __ldg(off + v));
 }
 
+constexpr uint32_t kEmpty = 0xffffffffu;
+
+// The subgraph induced on C = N+(v0), in shared memory:
+//   c[d]            the candidates (sorted vertex ids)
+//   hkey/hidx[T]    open-addressing hash of c: vertex id -> position (T = 2^logt >= 2d)
+//   rows[d * W]     bit j of row i set iff c[j] in N+(c[i])   (only j > i)
+//   rlo/rhi[d]      first / one-past-last non-zero word of each row
+struct Local {
+    uint32_t *c;
+    uint32_t *hkey;
+    uint16_t *hidx;
+    uint32_t *rows;
+    uint16_t *rlo, *rhi;
+    int d, W, logt;
+    __device__ __forceinline__ uint32_t slot(uint32_t x) const { return (x * 0x9E3779B1u) >> (32 - logt); }
+    __device__ __forceinline__ int find(uint32_t x) const {
+        const uint32_t mask = (1u << logt) - 1u;
+        uint32_t h = slot(x);
+        while (true) {
+            const uint32_t k = hkey[h];
+            if (k == x) return hidx[h];
+            if (k == kEmpty) return -1;
+            h = (h + 1) & mask;
+        }
+    }
+};
+
+// insert c[t] for t in [tid, d) step nthr (the table was set to kEmpty before a barrier)
+__device__ __forceinline__ void hash_insert(const Local &g, int tid, int nthr) {
+    const uint32_t mask = (1u << g.logt) - 1u;
+    for (int t = tid; t < g.d; t += nthr) {
+        const uint32_t x = g.c[t];
+        uint32_t h = g.slot(x);
+        while (atomicCAS(&g.hkey[h], kEmpty, x) != kEmpty) h = (h + 1) & mask;
+        g.hidx[h] = (uint16_t)t;
+    }
+}
+
 // Build rows [row_begin, d - 1) with stride row_step; the calling warp owns those rows.
-__device__ void build_rows(uint32_t *rows, int W, int d, const uint32_t *sC, const uint64_t *__restrict__ off,
-                           const uint32_t *__restrict__ adj, int row_begin, int row_step) {
+// Members of N+(c[i]) outside [c[i+1], c[d-1]] cannot be in C and are skipped.
+__device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                           int row_begin, int row_step) {
     const unsigned lane = lane_id();
-    const uint32_t hi_val = sC[d - 1];
+    const int d = g.d;
+    const uint32_t hi_val = g.c[d - 1];
     for (int i = row_begin; i < d - 1; i += row_step) {
-        const uint32_t v = sC[i];
+        const uint32_t v = g.c[i];
         const uint64_t b0 = __ldg(off + v);
         const uint32_t len = (uint32_t)(__ldg(off + v + 1) - b0);
         const uint32_t *L = adj + b0;
-        uint32_t start = lower_bound_u32(L, 0, len, sC[i + 1]);
-        uint32_t *row = rows + (size_t)i * W;
-        uint32_t lo = (uint32_t)i + 1;
+        const uint32_t start = lower_bound_u32(L, 0, len, g.c[i + 1]);
+        uint32_t *row = g.rows + (size_t)i * g.W;
         for (uint32_t b = start; b < len; b += 32) {
             const uint32_t idx = b + lane;
-            const uint32_t x = idx < len ? __ldg(L + idx) : 0xffffffffu;
-            uint32_t j = (uint32_t)d;
+            const uint32_t x = idx < len ? __ldg(L + idx) : kEmpty;
             if (x <= hi_val) {
-                j = lower_bound_plain(sC, lo, (uint32_t)d, x);
-                if (j < (uint32_t)d && sC[j] == x) atomicOr(row + (j >> 5), 1u << (j & 31));
+                const int j = g.find(x);
+                if (j >= 0) atomicOr(row + (j >> 5), 1u << (j & 31));
             }
-            const uint32_t xl = __shfl_sync(kFull, x, 31);
-            const uint32_t jl = __shfl_sync(kFull, j, 31);
-            if (xl >= hi_val) break;
-            lo = jl < (uint32_t)d ? jl : lo;
+            if (__shfl_sync(kFull, x, 31) >= hi_val) break;
         }
     }
 }
 
+// first / one-past-last non-zero word of rows [tid, d) step nthr
+__device__ __forceinline__ void row_extents(const Local &g, int tid, int nthr) {
+    for (int i = tid; i < g.d; i += nthr) {
+        const uint32_t *r = g.rows + (size_t)i * g.W;
+        int lo = g.W, hi = 0;
+        for (int w = (i + 1) >> 5; w < g.W; ++w) {
+            if (r[w]) {
+                lo = min(lo, w);
+                hi = w + 1;
+            }
+        }
+        g.rlo[i] = (uint16_t)(hi == 0 ? g.W : lo);
+        g.rhi[i] = (uint16_t)hi;
+    }
+}
+
 template <int K, bool STATS>
-__device__ __forceinline__ void process_item(const uint32_t *rows, int W, int i, int j, const uint32_t *sC,
-                                             const uint64_t *off, Acc &a) {
-    const uint32_t *ri = rows + (size_t)i * W;
-    const uint32_t *rj = rows + (size_t)j * W;
-    const int w0 = j >> 5;
+__device__ __forceinline__ void process_item(const Local &g, int i, int j, const uint64_t *off, Acc &a) {
+    const uint32_t *ri = g.rows + (size_t)i * g.W;
+    const uint32_t *rj = g.rows + (size_t)j * g.W;
+    const int lo = max((int)g.rlo[i], (int)g.rlo[j]);
+    const int hi = min((int)g.rhi[i], (int)g.rhi[j]);
     uint32_t s = 0;
-    for (int w = w0; w < W; ++w) s += __popc(ri[w] & rj[w]);
+    for (int w = lo; w < hi; ++w) s += __popc(ri[w] & rj[w]);
     if (STATS) {
         uint32_t pi = 0;
-        for (int w = 0; w < W; ++w) pi += __popc(ri[w]);
-        a.bytes += 4ull * ((uint64_t)pi + odeg(off, sC[j]) + s);
+        for (int w = g.rlo[i]; w < g.rhi[i]; ++w) pi += __popc(ri[w]);
+        a.bytes += 4ull * ((uint64_t)pi + odeg(off, g.c[j]) + s);
     }
     if (K == 4) {
         a.cnt += s;
         return;
     }
     a.t4 += s;
-    for (int w1 = w0; w1 < W; ++w1) {
+    for (int w1 = lo; w1 < hi; ++w1) {
         uint32_t m = ri[w1] & rj[w1];
         while (m) {
             const int l = (w1 << 5) + __ffs(m) - 1;
             m &= m - 1;
-            const uint32_t *rl = rows + (size_t)l * W;
+            const uint32_t *rl = g.rows + (size_t)l * g.W;
+            const int lo3 = max(lo, (int)g.rlo[l]);
+            const int hi3 = min(hi, (int)g.rhi[l]);
             uint32_t t = 0;
-            for (int w = l >> 5; w < W; ++w) t += __popc(ri[w] & rj[w] & rl[w]);
+            for (int w = lo3; w < hi3; ++w) t += __popc(ri[w] & rj[w] & rl[w]);
             a.cnt += t;
-            if (STATS) a.bytes += 4ull * ((uint64_t)s + odeg(off, sC[l]) + t);
+            if (STATS) a.bytes += 4ull * ((uint64_t)s + odeg(off, g.c[l]) + t);
         }
     }
 }
@@ -122,22 +175,22 @@ __device__ __forceinline__ void process_item(const uint32_t *rows, int W, int i,
 // Count over rows [row_begin, d) with stride row_step; (i, j) items are dealt to the
 // lanes of the calling warp in batches of 32.
 template <int K, bool STATS>
-__device__ void count_rows(const uint32_t *rows, int W, int d, const uint32_t *sC, const uint64_t *off,
-                           int row_begin, int row_step, Acc &a) {
+__device__ void count_rows(const Local &g, const uint64_t *off, int row_begin, int row_step, Acc &a) {
     const unsigned lane = lane_id();
-    int pc = 0;           // pending items held by lanes [0, pc)
+    int pc = 0;  // pending items held by lanes [0, pc)
     int my_i = 0, my_j = 0;
-    for (int i = row_begin; i < d; i += row_step) {
-        const uint32_t *ri = rows + (size_t)i * W;
+    for (int i = row_begin; i < g.d; i += row_step) {
+        const uint32_t *ri = g.rows + (size_t)i * g.W;
+        const int lo = g.rlo[i], hi = g.rhi[i];
         uint32_t pop = 0;
-        for (int w = (i + 1) >> 5; w < W; ++w) pop += __popc(ri[w]);
+        for (int w = lo; w < hi; ++w) pop += __popc(ri[w]);
         if (lane == 0) a.t3 += pop;
-        if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)d + odeg(off, sC[i]) + pop);
+        if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]) + pop);
         if (K == 3) {
             if (lane == 0) a.cnt += pop;
             continue;
         }
-        for (int ww = (i + 1) >> 5; ww < W; ++ww) {
+        for (int ww = lo; ww < hi; ++ww) {
             const uint32_t bits = ri[ww];
             const int c = __popc(bits);
             if (c == 0) continue;
@@ -147,7 +200,7 @@ __device__ void count_rows(const uint32_t *rows, int W, int d, const uint32_t *s
                 my_j = (ww << 5) + nth_set_bit(bits, q - pc);
             }
             if (pc + c >= 32) {
-                process_item<K, STATS>(rows, W, my_i, my_j, sC, off, a);
+                process_item<K, STATS>(g, my_i, my_j, off, a);
                 const int rem = pc + c - 32;
                 if (q < rem) {
                     my_i = i;
@@ -159,7 +212,7 @@ __device__ void count_rows(const uint32_t *rows, int W, int d, const uint32_t *s
             }
         }
     }
-    if (K > 3 && (int)lane < pc) process_item<K, STATS>(rows, W, my_i, my_j, sC, off, a);
+    if (K > 3 && (int)lane < pc) process_item<K, STATS>(g, my_i, my_j, off, a);
 }
 
 __device__ __forceinline__ void flush_acc(Acc &a, int K, uint64_t *out, uint64_t *phase_bytes) {
@@ -182,18 +235,30 @@ __device__ __forceinline__ void flush_acc(Acc &a, int K, uint64_t *out, uint64_t
 
 // Warp tier: one warp per start vertex with dmin <= d <= 64; vertices taken in descending id
 // order (heaviest first on the oriented DAG, whose ids are degree ranks).
+constexpr int kWarpHashLog = 7;  // 128-slot table per warp
 template <int K, bool STATS>
 __global__ void __launch_bounds__(256) clique_warp_kernel(const uint64_t *__restrict__ off,
                                                           const uint32_t *__restrict__ adj, uint32_t n,
                                                           uint32_t dmin, unsigned long long *queue,
                                                           uint64_t *out, uint64_t *phase_bytes) {
     constexpr int W = kWarpMax / 32;
+    constexpr int T = 1 << kWarpHashLog;
     __shared__ uint32_t s_c[8][kWarpMax];
     __shared__ uint32_t s_rows[8][kWarpMax * W];
+    __shared__ uint32_t s_hkey[8][T];
+    __shared__ uint16_t s_hidx[8][T];
+    __shared__ uint16_t s_rlo[8][kWarpMax], s_rhi[8][kWarpMax];
     const unsigned lane = lane_id();
     const int wib = threadIdx.x >> 5;
-    uint32_t *sC = s_c[wib];
-    uint32_t *rows = s_rows[wib];
+    Local g;
+    g.c = s_c[wib];
+    g.rows = s_rows[wib];
+    g.hkey = s_hkey[wib];
+    g.hidx = s_hidx[wib];
+    g.rlo = s_rlo[wib];
+    g.rhi = s_rhi[wib];
+    g.W = W;
+    g.logt = kWarpHashLog;
     Acc a = {0, 0, 0, 0, 0};
     constexpr uint32_t kChunk = 32;
     while (true) {
@@ -215,18 +280,36 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const uint64_t *__rest
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
             const uint32_t v0 = __shfl_sync(kFull, myv, src);
-            const int d = (int)__shfl_sync(kFull, myd, src);
+            g.d = (int)__shfl_sync(kFull, myd, src);
             const uint64_t b0 = __ldg(off + v0);
             __syncwarp();
-            for (int t = lane; t < kWarpMax; t += 32) sC[t] = t < d ? __ldg(adj + b0 + t) : 0xffffffffu;
-            for (int t = lane; t < kWarpMax * W; t += 32) rows[t] = 0;
+            for (int t = lane; t < kWarpMax; t += 32) g.c[t] = t < g.d ? __ldg(adj + b0 + t) : kEmpty;
+            for (int t = lane; t < kWarpMax * W; t += 32) g.rows[t] = 0;
+            for (int t = lane; t < T; t += 32) g.hkey[t] = kEmpty;
             __syncwarp();
-            if (d >= 2) build_rows(rows, W, d, sC, off, adj, 0, 1);
+            hash_insert(g, lane, 32);
             __syncwarp();
-            count_rows<K, STATS>(rows, W, d, sC, off, 0, 1, a);
+            if (g.d >= 2) build_rows(g, off, adj, 0, 1);
+            __syncwarp();
+            row_extents(g, lane, 32);
+            __syncwarp();
+            count_rows<K, STATS>(g, off, 0, 1, a);
         }
     }
     flush_acc(a, K, out, phase_bytes);
+}
+
+// shared-memory footprint of a block-tier launch serving out-degrees up to dcap
+__host__ __device__ __forceinline__ int block_logt(int dcap) {
+    int l = 5;
+    while ((1 << l) < 2 * dcap) ++l;
+    return l;
+}
+__host__ __device__ __forceinline__ size_t block_smem(int dcap) {
+    const size_t dp = (size_t)((dcap + 31) & ~31);
+    const size_t t = (size_t)1 << block_logt(dcap);
+    const size_t w = (size_t)((dcap + 31) / 32);
+    return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + dp * w * 4;
 }
 
 // Block tier: one block per start vertex from a degree-descending list.
@@ -234,31 +317,45 @@ template <int K, bool STATS>
 __global__ void clique_block_kernel(const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
                                     const uint32_t *__restrict__ list, uint32_t list_n, int dcap,
                                     unsigned long long *queue, uint64_t *out, uint64_t *phase_bytes) {
-    extern __shared__ uint32_t smem[];
+    extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_v0;
-    uint32_t *sC = smem;
-    uint32_t *rows = smem + ((dcap + 31) & ~31);
+    const int dp = (dcap + 31) & ~31;
+    const int logt = block_logt(dcap);
+    const int T = 1 << logt;
+    Local g;
+    g.c = smem;
+    g.hkey = smem + dp;
+    g.hidx = (uint16_t *)(g.hkey + T);
+    g.rlo = g.hidx + T;
+    g.rhi = g.rlo + dp;
+    g.rows = (uint32_t *)(g.rhi + dp);
+    g.logt = logt;
     const int warps = blockDim.x >> 5;
     const int wib = threadIdx.x >> 5;
     Acc a = {0, 0, 0, 0, 0};
     while (true) {
         if (threadIdx.x == 0) {
             const unsigned long long t = atomicAdd(queue, 1ull);
-            s_v0 = t < list_n ? list[t] : 0xffffffffu;
+            s_v0 = t < list_n ? list[t] : kEmpty;
         }
         __syncthreads();
         const uint32_t v0 = s_v0;
-        if (v0 == 0xffffffffu) break;
-        const int d = (int)odeg(off, v0);
-        const int W = (d + 31) >> 5;
-        if (threadIdx.x == 0) a.ext1 += (uint64_t)d;
+        if (v0 == kEmpty) break;
+        g.d = (int)odeg(off, v0);
+        g.W = (g.d + 31) >> 5;
+        if (threadIdx.x == 0) a.ext1 += (uint64_t)g.d;
         const uint64_t b0 = __ldg(off + v0);
-        for (int t = threadIdx.x; t < d; t += blockDim.x) sC[t] = __ldg(adj + b0 + t);
-        for (int t = threadIdx.x; t < d * W; t += blockDim.x) rows[t] = 0;
+        for (int t = threadIdx.x; t < g.d; t += blockDim.x) g.c[t] = __ldg(adj + b0 + t);
+        for (int t = threadIdx.x; t < g.d * g.W; t += blockDim.x) g.rows[t] = 0;
+        for (int t = threadIdx.x; t < T; t += blockDim.x) g.hkey[t] = kEmpty;
         __syncthreads();
-        build_rows(rows, W, d, sC, off, adj, wib, warps);
+        hash_insert(g, threadIdx.x, blockDim.x);
         __syncthreads();
-        count_rows<K, STATS>(rows, W, d, sC, off, wib, warps, a);
+        build_rows(g, off, adj, wib, warps);
+        __syncthreads();
+        row_extents(g, threadIdx.x, blockDim.x);
+        __syncthreads();
+        count_rows<K, STATS>(g, off, wib, warps, a);
         __syncthreads();
     }
     flush_acc(a, K, out, phase_bytes);
@@ -335,8 +432,9 @@ khz_status launch_all(const Graph &g, uint64_t *d_out, Workspace *ws, cudaStream
     mark(0, false);
     if (ls) ls->launches += 1;
     // block tiers, each list sorted by degree descending
-    const int tier_dcap[2] = {kMidMax, kBlockMax};
-    const int tier_threads[2] = {128, 512};
+    const int large_cap = (int)std::min<uint32_t>((uint32_t)kBlockMax, std::max<uint32_t>(g.max_degree, kMidMax + 1));
+    const int tier_dcap[2] = {kMidMax, large_cap};
+    const int tier_threads[2] = {256, 1024};
     for (int t = 0; t < 2; ++t) {
         const unsigned int cnt = h_counts[t];
         if (cnt == 0) continue;
@@ -344,7 +442,7 @@ khz_status launch_all(const Graph &g, uint64_t *d_out, Workspace *ws, cudaStream
         KHZ_CUDA(cub::DeviceRadixSort::SortPairsDescending(cub_tmp, cb, keys + (size_t)t * n, skeys,
                                                            vals + (size_t)t * n, svals, (int)cnt, 0, 32, s));
         const int dcap = tier_dcap[t];
-        const size_t smem = (size_t)((dcap + 31) & ~31) * 4 + (size_t)dcap * ((dcap + 31) / 32) * 4;
+        const size_t smem = block_smem(dcap);
         auto kern = clique_block_kernel<K, STATS>;
         KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;

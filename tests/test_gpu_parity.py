@@ -271,3 +271,53 @@ def test_graph_shape_detection_and_as_stored_semantics(graphs, khz_ctx):
         got, st = khz_ctx.count(dg, app)
         assert got == exp and st.num_extensions == ext, app
     dg.free()
+
+
+def test_bitmap_large_tier_matches_oracle(khz_ctx):
+    """A dense graph whose oriented out-degrees reach the large block tier (> 256)."""
+    from openkhuzdulgraph_b200 import khz
+    canon, n = orc.er(1500, 250000, seed=5)
+    sym = orc.symmetrize(canon)
+    off, adj = orc.csr(sym, n)
+    ooff, oadj, _ = orc.orient(off, adj)
+    assert int(np.diff(ooff).max()) > 256
+    og = khz_ctx.graph_from_edges(sym, n, orient=True)
+    try:
+        for app in ["kautomine_triangle", "kautomine_four_clique"]:
+            khz_ctx.set_config(engine=khz.ENGINE_BITMAP)
+            got, st = khz_ctx.count(og, app)
+            exp, ext, _ = orc.count(app, ooff, oadj)
+            assert got == exp and st.num_extensions == ext, app
+            assert st.phase_launches[2] == 1  # the large tier ran
+        khz_ctx.set_config(engine=khz.ENGINE_BITMAP)
+        b5, sb = khz_ctx.count(og, "kautomine_five_clique")
+        khz_ctx.set_config(engine=khz.ENGINE_DFS)
+        d5, sd = khz_ctx.count(og, "kautomine_five_clique")
+        assert b5 == d5 and sb.num_extensions == sd.num_extensions
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+        og.free()
+
+
+def test_bitmap_overflow_tier_complete_graph(khz_ctx):
+    """K_1250: out-degrees up to 1249 exceed the block tier, so the heaviest start vertices go to
+    the DFS engine; counts and NumExtensions follow from binomial coefficients."""
+    from math import comb
+    from openkhuzdulgraph_b200 import khz
+    n = 1250
+    iu = np.triu_indices(n, 1)
+    canon = np.stack([iu[0], iu[1]], axis=1).astype(np.uint32)
+    g = khz_ctx.graph_from_edges(orc.symmetrize(canon), n)
+    m = comb(n, 2)
+    try:
+        for engine in [khz.ENGINE_AUTO, khz.ENGINE_DFS]:
+            khz_ctx.set_config(engine=engine)
+            got, st = khz_ctx.count(g, "kautomine_triangle")
+            assert got == [comb(n, 3)] and st.num_extensions == n + m
+            got, st = khz_ctx.count(g, "kautomine_four_clique")
+            assert got == [comb(n, 4)] and st.num_extensions == n + m + comb(n, 3)
+            if engine == khz.ENGINE_AUTO:
+                assert st.phase_launches[3] == 1  # overflow start vertices ran on the DFS engine
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+        g.free()
