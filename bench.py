@@ -235,17 +235,23 @@ def ours(args, rank, world, local):
     pairs = torch.from_numpy(np.stack([src, adj_h], axis=1).reshape(-1).view(np.int32)).pin_memory()
     del src
     e2e_ms = []
+    e2e_parts = [0.0, 0.0, 0.0]  # build (upload + validate + CSR), count (+ result copy), free
     for i in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g2 = ctx.graph_from_edges(pairs, n, stream=sptr)
+        ta = time.perf_counter()
         c2, st2 = ctx.count(g2, APP, stream=sptr)
+        tb = time.perf_counter()
         g2.free()
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         assert c2 == ref_counts
         if i >= args.warmup:
             e2e_ms.append((t1 - t0) * 1000.0)
+            e2e_parts[0] += (ta - t0) * 1000.0 / args.steps
+            e2e_parts[1] += (tb - ta) * 1000.0 / args.steps
+            e2e_parts[2] += (t1 - tb) * 1000.0 / args.steps
     e2e_total = max_over_ranks(sum(e2e_ms), world, local)
     e2e_value = embeddings * world / (e2e_total / args.steps / 1000.0)
 
@@ -269,7 +275,8 @@ def ours(args, rank, world, local):
                        "embeddings_per_step": embeddings, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs (275 MB CSR) larger than L2; no flush"},
             "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": int(pairs.numel() * 4),
-                    "d2h_bytes_per_step": 8 * 8, "ms_per_step": e2e_total / args.steps},
+                    "d2h_bytes_per_step": 8 * 8, "ms_per_step": e2e_total / args.steps,
+                    "ms_build_count_free": e2e_parts},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": khz.Stats.PHASES[dom], "kernel_ms": dom_ms,

@@ -20,6 +20,27 @@
 
 namespace khz {
 
+static thread_local cudaMemPool_t t_pool = nullptr;
+static thread_local cudaStream_t t_stream = nullptr;
+
+AllocScope::AllocScope(cudaMemPool_t pool, cudaStream_t s) : prev_pool(t_pool), prev_stream(t_stream) {
+    t_pool = pool;
+    t_stream = s;
+}
+AllocScope::~AllocScope() {
+    t_pool = prev_pool;
+    t_stream = prev_stream;
+}
+cudaError_t dev_alloc(void **p, size_t bytes) {
+    if (t_pool) return cudaMallocFromPoolAsync(p, bytes, t_pool, t_stream);
+    return cudaMalloc(p, bytes);
+}
+void dev_free(void *p) {
+    if (!p) return;
+    if (t_pool) cudaFreeAsync(p, t_stream);
+    else cudaFree(p);
+}
+
 namespace {
 
 __global__ void validate_pairs_kernel(const uint32_t *__restrict__ pairs, uint64_t m, uint32_t n,
@@ -183,7 +204,7 @@ int num_sms() {
 template <typename T>
 khz_status dalloc(T **p, size_t count) {
     *p = nullptr;
-    cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(count, 1) * sizeof(T));
+    cudaError_t e = dev_alloc((void **)p, std::max<size_t>(count, 1) * sizeof(T));
     if (e != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of %llu bytes failed: %s", (unsigned long long)(count * sizeof(T)),
@@ -195,16 +216,14 @@ khz_status dalloc(T **p, size_t count) {
 
 struct DevBuf {
     void *p = nullptr;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
+    ~DevBuf() { dev_free(p); }
 };
 
 }  // namespace
 
 void free_graph_memory(Graph *g) {
-    if (g->off) cudaFree(g->off);
-    if (g->adj) cudaFree(g->adj);
+    dev_free(g->off);
+    dev_free(g->adj);
     g->off = nullptr;
     g->adj = nullptr;
 }
@@ -217,7 +236,7 @@ khz_status build_csr_from_device_pairs(const uint32_t *d_pairs, uint64_t m, uint
         return KHZ_ERR_FORMAT;
     }
     DevBuf flag;
-    KHZ_CUDA(cudaMalloc(&flag.p, sizeof(unsigned int) * 4));
+    KHZ_CUDA(dev_alloc(&flag.p, sizeof(unsigned int) * 4));
     KHZ_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(unsigned int) * 4, s));
     unsigned int hflags[4] = {0, 1, 1, 0};  // bad, not_upper, asym (unknown without validation)
     if (validate && m > 0) {
@@ -279,9 +298,9 @@ khz_status orient_graph(const Graph &in, Graph *outg, cudaStream_t s) {
     out.n = n;
     out.oriented = true;
     DevBuf keys, skeys, rank, tmp;
-    KHZ_CUDA(cudaMalloc(&keys.p, sizeof(uint64_t) * ((size_t)n + 1)));
-    KHZ_CUDA(cudaMalloc(&skeys.p, sizeof(uint64_t) * std::max<uint32_t>(n, 1)));
-    KHZ_CUDA(cudaMalloc(&rank.p, sizeof(uint32_t) * std::max<uint32_t>(n, 1)));
+    KHZ_CUDA(dev_alloc(&keys.p, sizeof(uint64_t) * ((size_t)n + 1)));
+    KHZ_CUDA(dev_alloc(&skeys.p, sizeof(uint64_t) * std::max<uint32_t>(n, 1)));
+    KHZ_CUDA(dev_alloc(&rank.p, sizeof(uint32_t) * std::max<uint32_t>(n, 1)));
     khz_status st = dalloc(&out.off, (size_t)n + 1);
     if (st) return st;
     if (n > 0) {
@@ -290,7 +309,7 @@ khz_status orient_graph(const Graph &in, Graph *outg, cudaStream_t s) {
         cub::DeviceRadixSort::SortKeys(nullptr, tb, (uint64_t *)keys.p, (uint64_t *)skeys.p, (int)n);
         size_t tb2 = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tb2, out.off, out.off, (int)n + 1);
-        KHZ_CUDA(cudaMalloc(&tmp.p, std::max(tb, tb2)));
+        KHZ_CUDA(dev_alloc(&tmp.p, std::max(tb, tb2)));
         KHZ_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, tb, (uint64_t *)keys.p, (uint64_t *)skeys.p, (int)n, 0, 64, s));
         rank_kernel<<<grid_for(n, sms), 256, 0, s>>>((uint64_t *)skeys.p, n, (uint32_t *)rank.p);
         const int wblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)n + 7) / 8, (uint64_t)sms * 16));
@@ -316,11 +335,11 @@ khz_status orient_graph(const Graph &in, Graph *outg, cudaStream_t s) {
         KHZ_CUDA(cudaGetLastError());
         if (m > 0) {
             DevBuf sorted, stmp;
-            KHZ_CUDA(cudaMalloc(&sorted.p, sizeof(uint32_t) * m));
+            KHZ_CUDA(dev_alloc(&sorted.p, sizeof(uint32_t) * m));
             size_t sb = 0;
             cub::DeviceSegmentedSort::SortKeys(nullptr, sb, out.adj, (uint32_t *)sorted.p, (int64_t)m, (int64_t)n,
                                                out.off, out.off + 1);
-            KHZ_CUDA(cudaMalloc(&stmp.p, std::max<size_t>(sb, 1)));
+            KHZ_CUDA(dev_alloc(&stmp.p, std::max<size_t>(sb, 1)));
             KHZ_CUDA(cub::DeviceSegmentedSort::SortKeys(stmp.p, sb, out.adj, (uint32_t *)sorted.p, (int64_t)m,
                                                         (int64_t)n, out.off, out.off + 1, s));
             KHZ_CUDA(cudaMemcpyAsync(out.adj, sorted.p, sizeof(uint32_t) * m, cudaMemcpyDeviceToDevice, s));
@@ -332,13 +351,13 @@ khz_status orient_graph(const Graph &in, Graph *outg, cudaStream_t s) {
         if (st) return st;
     }
     unsigned int *d_max = nullptr;
-    KHZ_CUDA(cudaMalloc(&d_max, sizeof(unsigned int)));
+    KHZ_CUDA(dev_alloc((void **)&d_max, sizeof(unsigned int)));
     cudaMemsetAsync(d_max, 0, sizeof(unsigned int), s);
     if (n > 0) max_degree_kernel<<<grid_for(n, sms), 256, 0, s>>>(out.off, n, d_max);
     unsigned int mx = 0;
     cudaMemcpyAsync(&mx, d_max, sizeof(mx), cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
-    cudaFree(d_max);
+    dev_free(d_max);
     if (e != cudaSuccess) {
         free_graph_memory(&out);
         return cuda_fail(e, "orientation");
@@ -368,8 +387,8 @@ khz_status generate_rmat(int scale, int edge_factor, double a, double b, double 
     base = (base ^ (base >> 27)) * 0x94D049BB133111EBULL;
     base ^= base >> 31;
     DevBuf keys, keys2, tmp, uniq_count, present, newid;
-    KHZ_CUDA(cudaMalloc(&keys.p, sizeof(uint64_t) * raw));
-    KHZ_CUDA(cudaMalloc(&keys2.p, sizeof(uint64_t) * raw));
+    KHZ_CUDA(dev_alloc(&keys.p, sizeof(uint64_t) * raw));
+    KHZ_CUDA(dev_alloc(&keys2.p, sizeof(uint64_t) * raw));
     rmat_kernel<<<grid_for(raw, sms), 256, 0, s>>>(scale, base, ta, tab, tabc, raw, (uint64_t *)keys.p);
     KHZ_CUDA(cudaGetLastError());
     size_t tb_sort = 0, tb_uniq = 0, tb_scan = 0;
@@ -382,8 +401,8 @@ khz_status generate_rmat(int scale, int edge_factor, double a, double b, double 
     size_t tb_sort2 = 0;
     cub::DeviceRadixSort::SortKeys(nullptr, tb_sort2, (uint64_t *)keys.p, (uint64_t *)keys2.p, (int64_t)(2 * raw));
     const size_t tb = std::max(std::max(tb_sort, tb_uniq), std::max(tb_scan, tb_sort2));
-    KHZ_CUDA(cudaMalloc(&tmp.p, tb));
-    KHZ_CUDA(cudaMalloc(&uniq_count.p, sizeof(uint64_t)));
+    KHZ_CUDA(dev_alloc(&tmp.p, tb));
+    KHZ_CUDA(dev_alloc(&uniq_count.p, sizeof(uint64_t)));
     size_t t1 = tb;
     KHZ_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, t1, (uint64_t *)keys.p, (uint64_t *)keys2.p, (int64_t)raw, 0, 64, s));
     t1 = tb;
@@ -399,8 +418,8 @@ khz_status generate_rmat(int scale, int edge_factor, double a, double b, double 
         if (last == ~0ull) nuniq -= 1;
     }
     const uint64_t m = nuniq;
-    KHZ_CUDA(cudaMalloc(&present.p, sizeof(uint32_t) * ((size_t)id_space + 1)));
-    KHZ_CUDA(cudaMalloc(&newid.p, sizeof(uint32_t) * ((size_t)id_space + 1)));
+    KHZ_CUDA(dev_alloc(&present.p, sizeof(uint32_t) * ((size_t)id_space + 1)));
+    KHZ_CUDA(dev_alloc(&newid.p, sizeof(uint32_t) * ((size_t)id_space + 1)));
     KHZ_CUDA(cudaMemsetAsync(present.p, 0, sizeof(uint32_t) * ((size_t)id_space + 1), s));
     if (m > 0) mark_present_kernel<<<grid_for(m, sms), 256, 0, s>>>((uint64_t *)keys.p, m, (uint32_t *)present.p);
     t1 = tb;
@@ -409,16 +428,16 @@ khz_status generate_rmat(int scale, int edge_factor, double a, double b, double 
     KHZ_CUDA(cudaMemcpyAsync(&n, (uint32_t *)newid.p + id_space, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     // symmetric keys: reuse keys2 (raw entries) when 2m fits, otherwise allocate
     DevBuf sym, sym_sorted;
-    KHZ_CUDA(cudaMalloc(&sym.p, sizeof(uint64_t) * std::max<uint64_t>(2 * m, 1)));
-    KHZ_CUDA(cudaMalloc(&sym_sorted.p, sizeof(uint64_t) * std::max<uint64_t>(2 * m, 1)));
+    KHZ_CUDA(dev_alloc(&sym.p, sizeof(uint64_t) * std::max<uint64_t>(2 * m, 1)));
+    KHZ_CUDA(dev_alloc(&sym_sorted.p, sizeof(uint64_t) * std::max<uint64_t>(2 * m, 1)));
     if (m > 0)
         relabel_sym_kernel<<<grid_for(m, sms), 256, 0, s>>>((uint64_t *)keys.p, m, (uint32_t *)newid.p,
                                                              (uint64_t *)sym.p);
     // release the raw buffers before the second sort
     KHZ_CUDA(cudaStreamSynchronize(s));
-    cudaFree(keys.p);
+    dev_free(keys.p);
     keys.p = nullptr;
-    cudaFree(keys2.p);
+    dev_free(keys2.p);
     keys2.p = nullptr;
     t1 = tb;
     if (m > 0)

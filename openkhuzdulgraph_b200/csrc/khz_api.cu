@@ -113,6 +113,7 @@ struct khz_ctx {
     uint64_t *d_extadd = nullptr;
     unsigned int *d_bad = nullptr;
     size_t rows_cap = 0;
+    cudaMemPool_t pool = nullptr;  // graphs and temporaries (keeps up to 4 GiB cached between calls)
     std::mutex mu;
 };
 
@@ -175,6 +176,7 @@ khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
     }
     if (g->oriented_view == 0) {
         Graph o;
+        AllocScope scope(ctx->pool, s);
         khz_status st = orient_graph(*g, &o, s);
         if (st) return st;
         khz_graph oh = add_graph(ctx, o);
@@ -390,6 +392,18 @@ khz_status khz_ctx_create(int device, khz_ctx **out) {
     KHZ_CUDA(cudaSetDevice(device));
     khz_ctx *c = new khz_ctx();
     c->device = device;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        set_error("cudaMemPoolCreate failed");
+        return KHZ_ERR_CUDA;
+    }
+    uint64_t keep = 4ull << 30;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     c->cfg.engine = KHZ_ENGINE_AUTO;
     c->cfg.dfs_warps_per_sm = 16;
     c->cfg.dfs_chunk = 8;
@@ -411,8 +425,13 @@ khz_status khz_ctx_destroy(khz_ctx *ctx) {
     if (!ctx) return KHZ_OK;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
-    for (size_t i = 0; i < ctx->graphs.size(); ++i)
-        if (ctx->live[i]) free_graph_memory(&ctx->graphs[i]);
+    {
+        AllocScope scope(ctx->pool, nullptr);
+        for (size_t i = 0; i < ctx->graphs.size(); ++i)
+            if (ctx->live[i]) free_graph_memory(&ctx->graphs[i]);
+    }
+    cudaDeviceSynchronize();
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     if (ctx->ws.slots) cudaFree(ctx->ws.slots);
     if (ctx->ws.counters) cudaFree(ctx->ws.counters);
     if (ctx->ws.tmp) cudaFree(ctx->ws.tmp);
@@ -464,10 +483,11 @@ khz_status khz_graph_from_edges(khz_ctx *ctx, const uint32_t *pairs, uint64_t m,
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
+    AllocScope scope(ctx->pool, s);
     const uint32_t *d_pairs = pairs;
     void *tmp = nullptr;
     if (!(flags & KHZ_EDGES_ON_DEVICE) && m > 0) {
-        cudaError_t e = cudaMalloc(&tmp, sizeof(uint32_t) * 2 * m);
+        cudaError_t e = dev_alloc(&tmp, sizeof(uint32_t) * 2 * m);
         if (e != cudaSuccess) {
             cudaGetLastError();
             set_error("device allocation for %llu edges failed", (unsigned long long)m);
@@ -475,14 +495,14 @@ khz_status khz_graph_from_edges(khz_ctx *ctx, const uint32_t *pairs, uint64_t m,
         }
         e = cudaMemcpyAsync(tmp, pairs, sizeof(uint32_t) * 2 * m, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess) {
-            cudaFree(tmp);
+            dev_free(tmp);
             return cuda_fail(e, "edge upload");
         }
         d_pairs = (const uint32_t *)tmp;
     }
     Graph g;
     st = build_csr_from_device_pairs(d_pairs, m, n, !(flags & KHZ_UNCHECKED), &g, s);
-    if (tmp) cudaFree(tmp);
+    if (tmp) dev_free(tmp);
     if (st) return st;
     if (flags & KHZ_ORIENT) {
         Graph o;
@@ -554,6 +574,7 @@ khz_status khz_graph_orient(khz_ctx *ctx, khz_graph in, khz_graph *out, void *st
         return KHZ_ERR_ARG;
     }
     Graph o;
+    AllocScope scope(ctx->pool, (cudaStream_t)stream);
     st = orient_graph(*g, &o, (cudaStream_t)stream);
     if (st) return st;
     *out = add_graph(ctx, o);
@@ -573,6 +594,7 @@ khz_status khz_graph_generate_rmat(khz_ctx *ctx, int scale, int edge_factor, dou
         return KHZ_ERR_ARG;
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
+    AllocScope scope(ctx->pool, (cudaStream_t)stream);
     Graph g;
     st = generate_rmat(scale, edge_factor, a, b, c, seed, &g, (cudaStream_t)stream);
     if (st) return st;
@@ -666,6 +688,9 @@ khz_status khz_graph_free(khz_ctx *ctx, khz_graph h) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     Graph *g = get_graph(ctx, h);
     if (!g) return KHZ_ERR_ARG;
+    // work on any stream may still read the graph: order the release after all of it
+    KHZ_CUDA(cudaDeviceSynchronize());
+    AllocScope scope(ctx->pool, nullptr);
     const khz_graph ov = g->oriented_view;
     free_graph_memory(g);
     ctx->live[h - 1] = false;

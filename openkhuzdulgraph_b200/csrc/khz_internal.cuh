@@ -107,6 +107,18 @@ struct Workspace {
     uint64_t pinned_bytes = 0;
 };
 
+// Device allocation for graphs and temporaries: from the context's stream-ordered pool when an
+// AllocScope is active on this thread (cudaMallocFromPoolAsync / cudaFreeAsync on its stream),
+// plain cudaMalloc / cudaFree otherwise.
+struct AllocScope {
+    AllocScope(cudaMemPool_t pool, cudaStream_t s);
+    ~AllocScope();
+    cudaMemPool_t prev_pool;
+    cudaStream_t prev_stream;
+};
+cudaError_t dev_alloc(void **p, size_t bytes);
+void dev_free(void *p);
+
 void set_error(const char *fmt, ...);
 khz_status cuda_fail(cudaError_t e, const char *what);
 
