@@ -10,6 +10,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -33,7 +34,7 @@ def _newer(target, deps):
 def build(verbose=False, ptxas_verbose=False):
     os.makedirs(OBJ, exist_ok=True)
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
-    objs = []
+    objs, cmds = [], []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
@@ -41,7 +42,10 @@ def build(verbose=False, ptxas_verbose=False):
             cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.check_call(cmd)
+            cmds.append(cmd)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     if _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         if verbose:
