@@ -165,6 +165,19 @@ typedef struct khz_job {
 khz_status khz_count_batch(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64_t *counts,
                            uint64_t *num_ext, khz_stats *stats, void *stream);
 
+/* A prepared batch: device tables and scratch are built once, the launch sequence (one bitmap
+ * launch sequence for the clique jobs, one persistent DFS launch for the rest, a finalize kernel)
+ * has no host synchronisation and, with KHZ_BATCH_CUDA_GRAPH, is captured into a CUDA graph and
+ * replayed by khz_batch_launch.  Results of the last launch: khz_batch_wait. */
+#define KHZ_BATCH_CUDA_GRAPH 0x1u
+typedef struct khz_batch khz_batch;
+khz_status khz_batch_create(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint32_t flags, khz_batch **out,
+                            void *stream);
+khz_status khz_batch_launch(khz_batch *batch, void *stream);
+/* counts: n_jobs * KHZ_MAX_COUNTS uint64; num_ext: n_jobs uint64 or NULL; blocks until ready */
+khz_status khz_batch_wait(khz_batch *batch, uint64_t *counts, uint64_t *num_ext, void *stream);
+khz_status khz_batch_destroy(khz_batch *batch);
+
 /* ---- VertexSet algebra as a batch (test / tool entry) ----------------------------- */
 /* VertexSet::intersect_with / subtracted_by / intersect_and_count / bounded_* and the
  * trims (vertex_set.cc:20-184, utilities.h:64-86) over n_pairs independent pairs of

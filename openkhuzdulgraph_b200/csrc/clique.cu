@@ -14,11 +14,12 @@
 // popcounts: n + m + #triangles (+ #4-cliques for k = 5).  The instrumented variant
 // also sums the schedule's algorithmic bytes 4 * (|A| + |B| + |A n B|) per set op.
 //
-// Tiers by out-degree d of v0: one warp per v0 for d <= 64 (rows of 2 words), one
-// block per v0 for 64 < d <= kBlockMax (rows in up to ~195 KB of shared memory, block
-// size chosen per tier); larger d are left to the DFS engine.  Blocks and warps take
-// start vertices from atomic queues, heaviest first.
-#include <cub/cub.cuh>
+// One launch sequence serves many (graph, clique app) jobs: their start vertices form one
+// global index space.  Tiers by out-degree d of v0: one warp per v0 for d <= 64 (rows of 2
+// words), one block per v0 for 64 < d <= 256 and 256 < d <= kBlockMax (rows in up to ~219 KB
+// of shared memory, sized from the largest out-degree of the batch); larger d are left to the
+// DFS engine.  Device-side classification sorts the block-tier start vertices into degree
+// buckets, heaviest bucket first, so nothing waits on the host between launches.
 #include <cuda_runtime.h>
 
 #include "khz_internal.cuh"
@@ -51,7 +52,7 @@ __device__ __forceinline__ int nth_set_bit(uint32_t x, int n) {
 }
 
 struct Acc {
-    uint64_t cnt, t3, t4, bytes, ext1;  // ext1: level-1 extensions (v0, v1) of the processed v0s
+    uint64_t cnt, t3, t4, bytes;
 };
 
 __device__ __forceinline__ uint32_t odeg(const uint64_t *off, uint32_t v) {
@@ -138,8 +139,8 @@ __device__ __forceinline__ void row_extents(const Local &g, int tid, int nthr) {
     }
 }
 
-template <int K, bool STATS>
-__device__ __forceinline__ void process_item(const Local &g, int i, int j, const uint64_t *off, Acc &a) {
+template <bool STATS>
+__device__ __forceinline__ void process_item(const Local &g, int K, int i, int j, const uint64_t *off, Acc &a) {
     const uint32_t *ri = g.rows + (size_t)i * g.W;
     const uint32_t *rj = g.rows + (size_t)j * g.W;
     const int lo = max((int)g.rlo[i], (int)g.rlo[j]);
@@ -172,10 +173,10 @@ __device__ __forceinline__ void process_item(const Local &g, int i, int j, const
     }
 }
 
-// Count over rows [row_begin, d) with stride row_step; (i, j) items are dealt to the
-// lanes of the calling warp in batches of 32.
-template <int K, bool STATS>
-__device__ void count_rows(const Local &g, const uint64_t *off, int row_begin, int row_step, Acc &a) {
+// Count over rows [row_begin, d) with stride row_step for a k-clique job; (i, j) items are dealt
+// to the lanes of the calling warp in batches of 32 (k is warp-uniform: one start vertex at a time).
+template <bool STATS>
+__device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, Acc &a) {
     const unsigned lane = lane_id();
     int pc = 0;  // pending items held by lanes [0, pc)
     int my_i = 0, my_j = 0;
@@ -200,7 +201,7 @@ __device__ void count_rows(const Local &g, const uint64_t *off, int row_begin, i
                 my_j = (ww << 5) + nth_set_bit(bits, q - pc);
             }
             if (pc + c >= 32) {
-                process_item<K, STATS>(g, my_i, my_j, off, a);
+                process_item<STATS>(g, K, my_i, my_j, off, a);
                 const int rem = pc + c - 32;
                 if (q < rem) {
                     my_i = i;
@@ -212,35 +213,49 @@ __device__ void count_rows(const Local &g, const uint64_t *off, int row_begin, i
             }
         }
     }
-    if (K > 3 && (int)lane < pc) process_item<K, STATS>(g, my_i, my_j, off, a);
+    if (K > 3 && (int)lane < pc) process_item<STATS>(g, K, my_i, my_j, off, a);
 }
 
-__device__ __forceinline__ void flush_acc(Acc &a, int K, uint64_t *out, uint64_t *phase_bytes) {
+// warp reduction of the accumulator and one atomicAdd per counter into the job's row
+__device__ __forceinline__ void flush_acc(Acc &a, int K, uint64_t *row, uint64_t *phase_bytes) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a.cnt += __shfl_down_sync(kFull, a.cnt, o);
         a.t3 += __shfl_down_sync(kFull, a.t3, o);
         a.t4 += __shfl_down_sync(kFull, a.t4, o);
         a.bytes += __shfl_down_sync(kFull, a.bytes, o);
-        a.ext1 += __shfl_down_sync(kFull, a.ext1, o);
     }
     if (lane_id() == 0) {
-        const uint64_t ext = a.ext1 + (K >= 4 ? a.t3 : 0) + (K >= 5 ? a.t4 : 0);
-        if (a.cnt) atomicAdd((unsigned long long *)&out[0], (unsigned long long)a.cnt);
-        if (ext) atomicAdd((unsigned long long *)&out[KHZ_MAX_COUNTS], (unsigned long long)ext);
-        if (a.bytes) atomicAdd((unsigned long long *)&out[KHZ_MAX_COUNTS + 1], (unsigned long long)a.bytes);
+        // NumExtensions beyond levels 0 and 1: the scattered triangles (k >= 4) and 4-cliques (k = 5)
+        const uint64_t ext = (K >= 4 ? a.t3 : 0) + (K >= 5 ? a.t4 : 0);
+        if (a.cnt) atomicAdd((unsigned long long *)&row[0], (unsigned long long)a.cnt);
+        if (ext) atomicAdd((unsigned long long *)&row[KHZ_MAX_COUNTS], (unsigned long long)ext);
+        if (a.bytes) atomicAdd((unsigned long long *)&row[KHZ_MAX_COUNTS + 1], (unsigned long long)a.bytes);
         if (a.bytes && phase_bytes) atomicAdd((unsigned long long *)phase_bytes, (unsigned long long)a.bytes);
     }
+    a = Acc{0, 0, 0, 0};
 }
 
-// Warp tier: one warp per start vertex with dmin <= d <= 64; vertices taken in descending id
-// order (heaviest first on the oriented DAG, whose ids are degree ranks).
+// job of a global start-vertex index (jobs sorted by vbase)
+__device__ __forceinline__ int job_of(const BJob *jobs, int n_jobs, uint64_t gv) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].vbase <= gv) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t *row_of(uint64_t *rows, const BJob &j) { return rows + (size_t)j.out_row * kRowWords; }
+
+// Warp tier: one warp per start vertex with dmin <= d <= 64 over all jobs' vertices, taken in
+// descending global index (per job: descending rank, i.e. heaviest first on the oriented DAG).
 constexpr int kWarpHashLog = 7;  // 128-slot table per warp
-template <int K, bool STATS>
-__global__ void __launch_bounds__(256) clique_warp_kernel(const uint64_t *__restrict__ off,
-                                                          const uint32_t *__restrict__ adj, uint32_t n,
-                                                          uint32_t dmin, unsigned long long *queue,
-                                                          uint64_t *out, uint64_t *phase_bytes) {
+template <bool STATS>
+__global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict__ jobs, int n_jobs,
+                                                          uint64_t n_total, uint32_t dmin,
+                                                          unsigned long long *queue, uint64_t *rows_out,
+                                                          uint64_t *phase_bytes) {
     constexpr int W = kWarpMax / 32;
     constexpr int T = 1 << kWarpHashLog;
     __shared__ uint32_t s_c[8][kWarpMax];
@@ -259,28 +274,38 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const uint64_t *__rest
     g.rhi = s_rhi[wib];
     g.W = W;
     g.logt = kWarpHashLog;
-    Acc a = {0, 0, 0, 0, 0};
+    Acc a = {0, 0, 0, 0};
+    int cur_job = -1;
     constexpr uint32_t kChunk = 32;
     while (true) {
         unsigned long long c0 = 0;
         if (lane == 0) c0 = atomicAdd(queue, (unsigned long long)kChunk);
         c0 = __shfl_sync(kFull, c0, 0);
-        if (c0 >= n) break;
-        const uint32_t c1 = (uint32_t)min((unsigned long long)n, c0 + kChunk);
-        // vertex candidates of this chunk, one per lane
-        const uint32_t myc = (uint32_t)c0 + lane;
+        if (c0 >= n_total) break;
+        const unsigned long long c1 = min((unsigned long long)n_total, c0 + kChunk);
+        // one candidate start vertex per lane
+        const unsigned long long myc = c0 + lane;
         uint32_t myv = 0, myd = 0;
+        int myj = 0;
         if (myc < c1) {
-            myv = n - 1 - myc;
-            myd = odeg(off, myv);
+            const uint64_t gv = n_total - 1 - myc;
+            myj = job_of(jobs, n_jobs, gv);
+            myv = (uint32_t)(gv - jobs[myj].vbase);
+            myd = odeg(jobs[myj].off, myv);
         }
-        if (myc < c1 && myd <= (uint32_t)kWarpMax) a.ext1 += myd;
         unsigned todo = __ballot_sync(kFull, myc < c1 && myd >= dmin && myd <= (uint32_t)kWarpMax);
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
             const uint32_t v0 = __shfl_sync(kFull, myv, src);
+            const int j = __shfl_sync(kFull, myj, src);
             g.d = (int)__shfl_sync(kFull, myd, src);
+            if (j != cur_job) {
+                if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
+                cur_job = j;
+            }
+            const uint64_t *off = jobs[j].off;
+            const uint32_t *adj = jobs[j].adj;
             const uint64_t b0 = __ldg(off + v0);
             __syncwarp();
             for (int t = lane; t < kWarpMax; t += 32) g.c[t] = t < g.d ? __ldg(adj + b0 + t) : kEmpty;
@@ -293,10 +318,10 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const uint64_t *__rest
             __syncwarp();
             row_extents(g, lane, 32);
             __syncwarp();
-            count_rows<K, STATS>(g, off, 0, 1, a);
+            count_rows<STATS>(g, jobs[j].k, off, 0, 1, a);
         }
     }
-    flush_acc(a, K, out, phase_bytes);
+    if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
 }
 
 // shared-memory footprint of a block-tier launch serving out-degrees up to dcap
@@ -312,13 +337,15 @@ __host__ __device__ __forceinline__ size_t block_smem(int dcap) {
     return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + dp * w * 4;
 }
 
-// Block tier: one block per start vertex from a degree-descending list.
-template <int K, bool STATS>
-__global__ void clique_block_kernel(const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
-                                    const uint32_t *__restrict__ list, uint32_t list_n, int dcap,
-                                    unsigned long long *queue, uint64_t *out, uint64_t *phase_bytes) {
+// Block tier: one block per start vertex; the list holds global start-vertex indices, heaviest
+// degree bucket first, and its length is read from device memory.
+template <bool STATS>
+__global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ list,
+                                    const unsigned int *__restrict__ list_len, int dcap, unsigned long long *queue,
+                                    uint64_t *rows_out, uint64_t *phase_bytes) {
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_v0;
+    __shared__ int s_job;
     const int dp = (dcap + 31) & ~31;
     const int logt = block_logt(dcap);
     const int T = 1 << logt;
@@ -332,18 +359,33 @@ __global__ void clique_block_kernel(const uint64_t *__restrict__ off, const uint
     g.logt = logt;
     const int warps = blockDim.x >> 5;
     const int wib = threadIdx.x >> 5;
-    Acc a = {0, 0, 0, 0, 0};
+    const unsigned int n_list = *list_len;
+    Acc a = {0, 0, 0, 0};
+    int cur_job = -1;
     while (true) {
         if (threadIdx.x == 0) {
             const unsigned long long t = atomicAdd(queue, 1ull);
-            s_v0 = t < list_n ? list[t] : kEmpty;
+            if (t < n_list) {
+                const uint64_t gv = list[t];
+                const int j = job_of(jobs, n_jobs, gv);
+                s_job = j;
+                s_v0 = (uint32_t)(gv - jobs[j].vbase);
+            } else {
+                s_job = -1;
+            }
         }
         __syncthreads();
+        const int j = s_job;
+        if (j < 0) break;
         const uint32_t v0 = s_v0;
-        if (v0 == kEmpty) break;
+        if (j != cur_job) {
+            if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
+            cur_job = j;
+        }
+        const uint64_t *off = jobs[j].off;
+        const uint32_t *adj = jobs[j].adj;
         g.d = (int)odeg(off, v0);
         g.W = (g.d + 31) >> 5;
-        if (threadIdx.x == 0) a.ext1 += (uint64_t)g.d;
         const uint64_t b0 = __ldg(off + v0);
         for (int t = threadIdx.x; t < g.d; t += blockDim.x) g.c[t] = __ldg(adj + b0 + t);
         for (int t = threadIdx.x; t < g.d * g.W; t += blockDim.x) g.rows[t] = 0;
@@ -355,66 +397,141 @@ __global__ void clique_block_kernel(const uint64_t *__restrict__ off, const uint
         __syncthreads();
         row_extents(g, threadIdx.x, blockDim.x);
         __syncthreads();
-        count_rows<K, STATS>(g, off, wib, warps, a);
+        count_rows<STATS>(g, jobs[j].k, off, wib, warps, a);
         __syncthreads();
     }
-    flush_acc(a, K, out, phase_bytes);
+    if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
 }
 
-__global__ void classify_kernel(const uint64_t *__restrict__ off, uint32_t n, uint32_t *keys, uint32_t *vals,
-                                unsigned int *counts) {
-    // counts[0]: mid tier (64, 256], counts[1]: large tier (256, kBlockMax], counts[2]: overflow
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const uint32_t d = odeg(off, v);
-        int t = -1;
-        if (d > kWarpMax && d <= kMidMax) t = 0;
-        else if (d > kMidMax && d <= kBlockMax) t = 1;
-        else if (d > kBlockMax) t = 2;
-        if (t >= 0) {
-            const unsigned int pos = atomicAdd(&counts[t], 1u);
-            keys[(size_t)t * n + pos] = d;
-            vals[(size_t)t * n + pos] = v;
+// Degree buckets of the block tiers, heaviest first within each list:
+//   mid list   = (128, 256] then (64, 128]
+//   large list = (1024, kBlockMax] then (512, 1024] then (256, 512]
+// Bucket 5 = overflow (left to the DFS engine), -1 = warp tier.
+__device__ __forceinline__ int bucket_of(uint32_t d) {
+    if (d <= (uint32_t)kWarpMax) return -1;
+    if (d <= 128) return 0;
+    if (d <= (uint32_t)kMidMax) return 1;
+    if (d <= 512) return 2;
+    if (d <= 1024) return 3;
+    if (d <= (uint32_t)kBlockMax) return 4;
+    return 5;
+}
+
+// classification counters (unsigned int): [0..5] bucket sizes, [6..11] cursors, [12..17] list
+// positions of each bucket, [18] mid list length, [19] large list length
+constexpr int kCntCursor = 6, kCntBase = 12, kCntMidLen = 18, kCntLargeLen = 19;
+
+// pass 1: bucket sizes, and the level-1 extensions (v0, v1) of every start vertex this engine
+// serves (the reference counts one extension per scattered v1, engine.cc:924)
+__global__ void classify_count_kernel(const BJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
+                                      unsigned int *cnt, uint64_t *rows_out) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: whole warps iterate together
+    for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < ((n_total + 31) & ~31ull);
+         gv += stride) {
+        int b = -2, j = -1;
+        uint32_t d = 0;
+        if (gv < n_total) {
+            j = job_of(jobs, n_jobs, gv);
+            d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
+            b = bucket_of(d);
         }
+        if (b >= 0 && b < 5) atomicAdd(&cnt[b], 1u);
+        // one atomic per distinct job per warp
+        const unsigned peers = __match_any_sync(kFull, j);
+        const uint64_t mine = (j >= 0 && b != 5) ? d : 0;
+        uint64_t sum = 0;
+        for (int l = 0; l < 32; ++l) {
+            const uint64_t v = __shfl_sync(kFull, mine, l);
+            if ((peers >> l) & 1u) sum += v;
+        }
+        if (j >= 0 && (int)lane_id() == __ffs(peers) - 1 && sum)
+            atomicAdd((unsigned long long *)&row_of(rows_out, jobs[j])[KHZ_MAX_COUNTS], (unsigned long long)sum);
     }
 }
 
-template <int K, bool STATS>
-khz_status launch_all(const Graph &g, uint64_t *d_out, Workspace *ws, cudaStream_t s, LaunchStats *ls,
-                      uint32_t *n_overflow) {
-    int dev = 0, sms = 0;
-    KHZ_CUDA(cudaGetDevice(&dev));
-    KHZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const uint32_t n = g.n;
-    // temp layout: keys[3n], vals[3n], sorted keys/vals [n], counts, cub temp
-    size_t cub_bytes = 0;
-    cub::DeviceRadixSort::SortPairsDescending(nullptr, cub_bytes, (uint32_t *)nullptr, (uint32_t *)nullptr,
-                                              (uint32_t *)nullptr, (uint32_t *)nullptr, (int)std::max(n, 1u));
-    const size_t lists = (size_t)3 * std::max(n, 1u) * sizeof(uint32_t);
-    const size_t sorted = (size_t)std::max(n, 1u) * sizeof(uint32_t);
-    const size_t need = 2 * lists + 2 * sorted + 256 + cub_bytes + 256;
-    if (ws->tmp_bytes < need) {
-        if (ws->tmp) cudaFree(ws->tmp);
-        ws->tmp = nullptr;
-        ws->tmp_bytes = 0;
-        KHZ_CUDA(cudaMalloc(&ws->tmp, need));
-        ws->tmp_bytes = need;
+__global__ void classify_prefix_kernel(unsigned int *cnt) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    cnt[kCntBase + 1] = 0;  // mid list: bucket 1 then 0
+    cnt[kCntBase + 0] = cnt[1];
+    cnt[kCntMidLen] = cnt[0] + cnt[1];
+    cnt[kCntBase + 4] = 0;  // large list: 4, 3, 2
+    cnt[kCntBase + 3] = cnt[4];
+    cnt[kCntBase + 2] = cnt[4] + cnt[3];
+    cnt[kCntLargeLen] = cnt[2] + cnt[3] + cnt[4];
+}
+
+// pass 2: write each block-tier start vertex into its list
+__global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
+                                      unsigned int *cnt, uint32_t *mid_list, uint32_t *large_list) {
+    for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < n_total;
+         gv += (uint64_t)gridDim.x * blockDim.x) {
+        const int j = job_of(jobs, n_jobs, gv);
+        const uint32_t d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
+        const int b = bucket_of(d);
+        if (b < 0 || b >= 5) continue;
+        const unsigned int pos = cnt[kCntBase + b] + atomicAdd(&cnt[kCntCursor + b], 1u);
+        if (b <= 1) mid_list[pos] = (uint32_t)gv;
+        else large_list[pos] = (uint32_t)gv;
     }
-    char *p = (char *)ws->tmp;
-    uint32_t *keys = (uint32_t *)p; p += lists;
-    uint32_t *vals = (uint32_t *)p; p += lists;
-    uint32_t *skeys = (uint32_t *)p; p += sorted;
-    uint32_t *svals = (uint32_t *)p; p += sorted;
-    unsigned int *tier_counts = (unsigned int *)p; p += 256;
-    void *cub_tmp = p;
-    unsigned long long *queues = (unsigned long long *)ws->counters;  // [0] warp, [1] mid, [2] large
-    KHZ_CUDA(cudaMemsetAsync(tier_counts, 0, 16, s));
-    KHZ_CUDA(cudaMemsetAsync(queues, 0, 4 * sizeof(unsigned long long), s));
-    classify_kernel<<<sms * 4, 256, 0, s>>>(g.off, n, keys, vals, tier_counts);
-    KHZ_CUDA(cudaGetLastError());
-    unsigned int h_counts[3];
-    KHZ_CUDA(cudaMemcpyAsync(h_counts, tier_counts, sizeof(h_counts), cudaMemcpyDeviceToHost, s));
-    KHZ_CUDA(cudaStreamSynchronize(s));
-    if (ls) ls->launches += 1;
+}
+
+}  // namespace
+
+uint32_t bitmap_block_max_degree() { return kBlockMax; }
+
+size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap) {
+    return Arena::round(sizeof(BJob) * (size_t)std::max(n_jobs, 1)) +
+           2 * Arena::round(sizeof(uint32_t) * std::max<uint64_t>(list_cap, 1)) +
+           Arena::round(sizeof(unsigned int) * 32) + Arena::round(sizeof(unsigned long long) * 4);
+}
+
+khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
+                          Arena *arena, BitmapLaunch *bl, cudaStream_t s) {
+    BitmapLaunch L;
+    L.n_jobs = (int)jobs.size();
+    L.n_total = jobs.empty() ? 0 : jobs.back().vbase + jobs.back().n;
+    L.stats = stats;
+    if (L.n_total >= (1ull << 32)) {
+        set_error("a bitmap launch serves at most 2^32 - 1 start vertices (got %llu)", (unsigned long long)L.n_total);
+        return KHZ_ERR_ARG;
+    }
+    BJob *d_jobs = arena->take<BJob>(jobs.size());
+    L.mid_list = arena->take<uint32_t>(list_cap);
+    L.large_list = arena->take<uint32_t>(list_cap);
+    L.cnt = arena->take<unsigned int>(32);
+    L.queues = arena->take<unsigned long long>(4);
+    if (!d_jobs || !L.mid_list || !L.large_list || !L.cnt || !L.queues) {
+        set_error("bitmap launch arena too small");
+        return KHZ_ERR_OOM;
+    }
+    if (!jobs.empty())
+        KHZ_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(BJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+    L.d_jobs = d_jobs;
+    int dev = 0;
+    KHZ_CUDA(cudaGetDevice(&dev));
+    KHZ_CUDA(cudaDeviceGetAttribute(&L.sms, cudaDevAttrMultiProcessorCount, dev));
+    L.large_dcap = (int)std::min<uint32_t>((uint32_t)kBlockMax, std::max<uint32_t>(max_outdeg, kMidMax + 1));
+    L.has_mid = max_outdeg > (uint32_t)kWarpMax;
+    L.has_large = max_outdeg > (uint32_t)kMidMax;
+    const int dcaps[2] = {kMidMax, L.large_dcap};
+    const int threads[2] = {256, 1024};
+    for (int t = 0; t < 2; ++t) {
+        const size_t smem = block_smem(dcaps[t]);
+        auto kern = stats ? clique_block_kernel<true> : clique_block_kernel<false>;
+        KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
+        L.block_smem[t] = smem;
+        L.block_threads[t] = threads[t];
+        L.block_grid[t] = L.sms * std::max(per_sm, 1);
+        L.block_dcap[t] = dcaps[t];
+    }
+    *bl = L;
+    return KHZ_OK;
+}
+
+khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls) {
+    if (L.n_jobs == 0 || L.n_total == 0) return KHZ_OK;
     auto pb = [&](int phase) -> uint64_t * { return ls && ls->d_phase_bytes ? ls->d_phase_bytes + phase : nullptr; };
     auto mark = [&](int phase, bool begin) {
         if (!ls || !ls->ev_begin) return;
@@ -424,69 +541,43 @@ khz_status launch_all(const Graph &g, uint64_t *d_out, Workspace *ws, cudaStream
             ls->phase_launches[phase] += 1;
         }
     };
-    // warp tier
+    KHZ_CUDA(cudaMemsetAsync(L.cnt, 0, sizeof(unsigned int) * 32, s));
+    KHZ_CUDA(cudaMemsetAsync(L.queues, 0, sizeof(unsigned long long) * 4, s));
+    const int cgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 255) / 256, (uint64_t)L.sms * 8));
+    classify_count_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.cnt, d_rows);
+    if (L.has_mid) {
+        classify_prefix_kernel<<<1, 32, 0, s>>>(L.cnt);
+        classify_write_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.cnt, L.mid_list, L.large_list);
+    }
+    KHZ_CUDA(cudaGetLastError());
+    if (ls) ls->launches += L.has_mid ? 3 : 1;
     mark(0, true);
-    clique_warp_kernel<K, STATS><<<sms * 8, 256, 0, s>>>(g.off, g.adj, n, STATS ? 1u : 2u, &queues[0], d_out,
-                                                          pb(0));
+    if (L.stats)
+        clique_warp_kernel<true><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 1u, &L.queues[0], d_rows,
+                                                           pb(0));
+    else
+        clique_warp_kernel<false><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 2u, &L.queues[0], d_rows,
+                                                            pb(0));
     KHZ_CUDA(cudaGetLastError());
     mark(0, false);
     if (ls) ls->launches += 1;
-    // block tiers, each list sorted by degree descending
-    const int large_cap = (int)std::min<uint32_t>((uint32_t)kBlockMax, std::max<uint32_t>(g.max_degree, kMidMax + 1));
-    const int tier_dcap[2] = {kMidMax, large_cap};
-    const int tier_threads[2] = {256, 1024};
+    const bool run[2] = {L.has_mid, L.has_large};
     for (int t = 0; t < 2; ++t) {
-        const unsigned int cnt = h_counts[t];
-        if (cnt == 0) continue;
-        size_t cb = cub_bytes;
-        KHZ_CUDA(cub::DeviceRadixSort::SortPairsDescending(cub_tmp, cb, keys + (size_t)t * n, skeys,
-                                                           vals + (size_t)t * n, svals, (int)cnt, 0, 32, s));
-        const int dcap = tier_dcap[t];
-        const size_t smem = block_smem(dcap);
-        auto kern = clique_block_kernel<K, STATS>;
-        KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = 0;
-        KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tier_threads[t], smem));
-        if (per_sm < 1) per_sm = 1;
-        const int blocks = (int)std::min<size_t>((size_t)sms * per_sm, cnt);
+        if (!run[t]) continue;
+        const uint32_t *list = t == 0 ? L.mid_list : L.large_list;
+        const unsigned int *len = L.cnt + (t == 0 ? kCntMidLen : kCntLargeLen);
         mark(1 + t, true);
-        kern<<<blocks, tier_threads[t], smem, s>>>(g.off, g.adj, svals, cnt, dcap, &queues[1 + t], d_out,
-                                                   pb(1 + t));
+        if (L.stats)
+            clique_block_kernel<true><<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(
+                L.d_jobs, L.n_jobs, list, len, L.block_dcap[t], &L.queues[1 + t], d_rows, pb(1 + t));
+        else
+            clique_block_kernel<false><<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(
+                L.d_jobs, L.n_jobs, list, len, L.block_dcap[t], &L.queues[1 + t], d_rows, pb(1 + t));
         KHZ_CUDA(cudaGetLastError());
         mark(1 + t, false);
-        if (ls) ls->launches += 2;
+        if (ls) ls->launches += 1;
     }
-    *n_overflow = h_counts[2];
     return KHZ_OK;
-}
-
-}  // namespace
-
-uint32_t bitmap_block_max_degree() { return kBlockMax; }
-
-khz_status bitmap_clique_run(const Graph &g, int k, bool stats, int warp_max, int block_warps, uint64_t *d_out,
-                             Workspace *ws, cudaStream_t s, LaunchStats *ls, uint32_t *n_overflow) {
-    (void)warp_max;
-    (void)block_warps;
-    if (!g.oriented) {
-        set_error("bitmap clique engine needs an oriented graph");
-        return KHZ_ERR_ARG;
-    }
-    if (g.n == 0) {
-        *n_overflow = 0;
-        return KHZ_OK;
-    }
-    switch (k * 2 + (stats ? 1 : 0)) {
-        case 6: return launch_all<3, false>(g, d_out, ws, s, ls, n_overflow);
-        case 7: return launch_all<3, true>(g, d_out, ws, s, ls, n_overflow);
-        case 8: return launch_all<4, false>(g, d_out, ws, s, ls, n_overflow);
-        case 9: return launch_all<4, true>(g, d_out, ws, s, ls, n_overflow);
-        case 10: return launch_all<5, false>(g, d_out, ws, s, ls, n_overflow);
-        case 11: return launch_all<5, true>(g, d_out, ws, s, ls, n_overflow);
-        default:
-            set_error("bitmap clique engine supports k = 3, 4, 5 (got %d)", k);
-            return KHZ_ERR_ARG;
-    }
 }
 
 }  // namespace khz

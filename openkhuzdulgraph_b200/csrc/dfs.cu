@@ -288,61 +288,71 @@ khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_p
     return KHZ_OK;
 }
 
-khz_status dfs_run(const DfsJob *h_jobs, int n_jobs, const Plan *h_plans, int n_plans, uint32_t slot_cap,
-                   bool stats, int warps_per_sm, int chunk, uint64_t *d_out, Workspace *ws, cudaStream_t s,
-                   LaunchStats *ls) {
-    if (n_jobs <= 0) return KHZ_OK;
+namespace {
+constexpr int kDfsWarpsPerBlock = 8;
+int num_sms_dfs() {
     int dev = 0, sms = 0;
-    KHZ_CUDA(cudaGetDevice(&dev));
-    KHZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+int dfs_blocks(int warps_per_sm) {
     if (warps_per_sm <= 0) warps_per_sm = 16;
-    if (chunk <= 0) chunk = 8;
-    const int warps_per_block = 8;
-    const int blocks = sms * ((warps_per_sm + warps_per_block - 1) / warps_per_block);
-    const uint64_t total_warps = (uint64_t)blocks * warps_per_block;
-    slot_cap = (slot_cap + 31u) & ~31u;
-    if (slot_cap == 0) slot_cap = 32;
-    const uint64_t need_slots = total_warps * kNumSlots * slot_cap * sizeof(uint32_t);
-    if (ws->slot_bytes < need_slots) {
-        if (ws->slots) cudaFree(ws->slots);
-        ws->slots = nullptr;
-        ws->slot_bytes = 0;
-        cudaError_t e = cudaMalloc(&ws->slots, need_slots);
-        if (e != cudaSuccess) {
-            set_error("DFS scratch allocation of %llu bytes failed", (unsigned long long)need_slots);
-            return KHZ_ERR_OOM;
-        }
-        ws->slot_bytes = need_slots;
+    return num_sms_dfs() * ((warps_per_sm + kDfsWarpsPerBlock - 1) / kDfsWarpsPerBlock);
+}
+uint32_t round_cap(uint32_t slot_cap) { return slot_cap == 0 ? 32u : ((slot_cap + 31u) & ~31u); }
+}  // namespace
+
+uint64_t dfs_total_warps(int warps_per_sm) { return (uint64_t)dfs_blocks(warps_per_sm) * kDfsWarpsPerBlock; }
+
+size_t dfs_arena_bytes(int n_jobs, int n_plans, uint64_t total_warps, uint32_t slot_cap) {
+    return Arena::round(sizeof(DfsJob) * (size_t)std::max(n_jobs, 1)) +
+           Arena::round(sizeof(Plan) * (size_t)std::max(n_plans, 4)) +
+           Arena::round(total_warps * kNumSlots * round_cap(slot_cap) * sizeof(uint32_t)) +
+           Arena::round(sizeof(unsigned long long));
+}
+
+khz_status dfs_prepare(const std::vector<DfsJob> &jobs, const std::vector<Plan> &plans, uint32_t slot_cap,
+                       int warps_per_sm, int chunk, bool stats, Arena *arena, DfsLaunch *dl, cudaStream_t s) {
+    DfsLaunch L;
+    L.n_jobs = (int)jobs.size();
+    L.stats = stats;
+    L.chunk = chunk > 0 ? (uint32_t)chunk : 8u;
+    L.blocks = dfs_blocks(warps_per_sm);
+    L.threads = kDfsWarpsPerBlock * 32;
+    L.slot_cap = round_cap(slot_cap);
+    for (const auto &j : jobs) L.total_units = std::max(L.total_units, j.unit_begin + j.num_units);
+    DfsJob *d_jobs = arena->take<DfsJob>(jobs.size());
+    // the kernel stages the first four plans into shared memory: keep at least four readable
+    Plan *d_plans = arena->take<Plan>(std::max<size_t>(plans.size(), 4));
+    L.slots = arena->take<uint32_t>((size_t)L.blocks * kDfsWarpsPerBlock * kNumSlots * L.slot_cap);
+    L.queue = arena->take<unsigned long long>(1);
+    if (!d_jobs || !d_plans || !L.slots || !L.queue) {
+        set_error("DFS launch arena too small");
+        return KHZ_ERR_OOM;
     }
-    uint64_t total_units = 0;
-    for (int j = 0; j < n_jobs; ++j) total_units = std::max(total_units, h_jobs[j].unit_begin + h_jobs[j].num_units);
-    // job and plan tables go into the workspace's temp buffer
-    const size_t jobs_bytes = sizeof(DfsJob) * (size_t)n_jobs;
-    const size_t plans_bytes = sizeof(Plan) * (size_t)std::max(n_plans, 4);
-    const size_t need_tmp = jobs_bytes + plans_bytes + 256;
-    if (ws->tmp_bytes < need_tmp) {
-        if (ws->tmp) cudaFree(ws->tmp);
-        ws->tmp = nullptr;
-        ws->tmp_bytes = 0;
-        KHZ_CUDA(cudaMalloc(&ws->tmp, need_tmp));
-        ws->tmp_bytes = need_tmp;
-    }
-    char *tmp = (char *)ws->tmp;
-    DfsJob *d_jobs = (DfsJob *)tmp;
-    Plan *d_plans = (Plan *)(tmp + ((jobs_bytes + 255) & ~(size_t)255));
-    KHZ_CUDA(cudaMemcpyAsync(d_jobs, h_jobs, jobs_bytes, cudaMemcpyHostToDevice, s));
-    KHZ_CUDA(cudaMemsetAsync(d_plans, 0, plans_bytes, s));
-    KHZ_CUDA(cudaMemcpyAsync(d_plans, h_plans, sizeof(Plan) * n_plans, cudaMemcpyHostToDevice, s));
-    unsigned long long *queue = (unsigned long long *)ws->counters + 8;
-    KHZ_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
+    if (!jobs.empty())
+        KHZ_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(DfsJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+    KHZ_CUDA(cudaMemsetAsync(d_plans, 0, sizeof(Plan) * std::max<size_t>(plans.size(), 4), s));
+    if (!plans.empty())
+        KHZ_CUDA(cudaMemcpyAsync(d_plans, plans.data(), sizeof(Plan) * plans.size(), cudaMemcpyHostToDevice, s));
+    L.d_jobs = d_jobs;
+    L.d_plans = d_plans;
+    *dl = L;
+    return KHZ_OK;
+}
+
+khz_status dfs_enqueue(const DfsLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls) {
+    if (L.n_jobs == 0 || L.total_units == 0) return KHZ_OK;
+    KHZ_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(unsigned long long), s));
     uint64_t *pb = ls && ls->d_phase_bytes ? ls->d_phase_bytes + 3 : nullptr;
     if (ls && ls->ev_begin) cudaEventRecord(ls->ev_begin[3], s);
-    if (stats)
-        dfs_kernel<true><<<blocks, warps_per_block * 32, 0, s>>>(d_jobs, n_jobs, d_plans, total_units, chunk,
-                                                                 ws->slots, slot_cap, queue, d_out, pb);
+    if (L.stats)
+        dfs_kernel<true><<<L.blocks, L.threads, 0, s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk, L.slots,
+                                                        L.slot_cap, L.queue, d_rows, pb);
     else
-        dfs_kernel<false><<<blocks, warps_per_block * 32, 0, s>>>(d_jobs, n_jobs, d_plans, total_units, chunk,
-                                                                  ws->slots, slot_cap, queue, d_out, pb);
+        dfs_kernel<false><<<L.blocks, L.threads, 0, s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk,
+                                                         L.slots, L.slot_cap, L.queue, d_rows, pb);
     KHZ_CUDA(cudaGetLastError());
     if (ls && ls->ev_begin) {
         cudaEventRecord(ls->ev_end[3], s);

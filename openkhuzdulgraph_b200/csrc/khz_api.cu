@@ -5,7 +5,10 @@
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
 #include <mutex>
+#include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "khz_internal.cuh"
@@ -33,7 +36,6 @@ khz_status cuda_fail(cudaError_t e, const char *what) {
 
 namespace {
 
-constexpr int kRow = KHZ_MAX_COUNTS + 2;
 
 // divides the raw counters by the multiplicities and adds the host-known NumExtensions terms
 __global__ void finalize_kernel(const uint64_t *raw, int rows, const uint32_t *mult, const uint64_t *ext_add,
@@ -41,13 +43,13 @@ __global__ void finalize_kernel(const uint64_t *raw, int rows, const uint32_t *m
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
     for (int c = 0; c < KHZ_MAX_COUNTS; ++c) {
-        const uint64_t v = raw[(size_t)r * kRow + c];
+        const uint64_t v = raw[(size_t)r * kRowWords + c];
         const uint32_t mu = mult[(size_t)r * KHZ_MAX_COUNTS + c];
         if (mu > 1 && v % mu) atomicOr(bad, 1u);
-        out[(size_t)r * kRow + c] = mu > 1 ? v / mu : v;
+        out[(size_t)r * kRowWords + c] = mu > 1 ? v / mu : v;
     }
-    out[(size_t)r * kRow + KHZ_MAX_COUNTS] = raw[(size_t)r * kRow + KHZ_MAX_COUNTS] + ext_add[r];
-    out[(size_t)r * kRow + KHZ_MAX_COUNTS + 1] = raw[(size_t)r * kRow + KHZ_MAX_COUNTS + 1];
+    out[(size_t)r * kRowWords + KHZ_MAX_COUNTS] = raw[(size_t)r * kRowWords + KHZ_MAX_COUNTS] + ext_add[r];
+    out[(size_t)r * kRowWords + KHZ_MAX_COUNTS + 1] = raw[(size_t)r * kRowWords + KHZ_MAX_COUNTS + 1];
 }
 
 // VertexSet ops as a batch: one warp per pair (vertex_set.cc:20-184, utilities.h:64-86)
@@ -100,21 +102,49 @@ __global__ void setop_batch_kernel(int op, const uint64_t *a_off, const uint32_t
 
 using namespace khz;
 
+// A prepared counting launch over one or more (graph, app) jobs.  Device job tables, engine
+// scratch and counter rows live in one allocation owned by the plan, so plans are independent of
+// one another (different plans may run concurrently on different streams), and enqueueing a plan
+// involves no host synchronisation, so its launch sequence can be captured into a CUDA graph.
+struct BatchPlan {
+    int rows = 0;
+    std::vector<int> apps;
+    bool stats = false;
+    bool has_bitmap = false, has_dfs = false;
+    uint32_t engine = KHZ_ENGINE_DFS;
+    BitmapLaunch bl;
+    DfsLaunch dl;
+    void *mem = nullptr;
+    Arena arena;
+    uint64_t *d_raw = nullptr, *d_final = nullptr, *d_extadd = nullptr, *d_phase_bytes = nullptr;
+    uint32_t *d_mult = nullptr;
+    unsigned int *d_bad = nullptr;
+    uint64_t *h_final = nullptr;  // pinned: rows * kRowWords, then the bad flag
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~BatchPlan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (mem) cudaFree(mem);
+        if (h_final) cudaFreeHost(h_final);
+    }
+};
+
 struct khz_ctx {
     int device = 0;
     khz_config cfg{};
     std::vector<Graph> graphs;  // handle h -> graphs[h - 1]
     std::vector<bool> live;
-    Workspace ws;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ph_begin[kPhases] = {}, ph_end[kPhases] = {};
-    uint64_t *d_rows = nullptr;  // raw + final counter rows
-    uint32_t *d_mult = nullptr;
-    uint64_t *d_extadd = nullptr;
-    unsigned int *d_bad = nullptr;
-    size_t rows_cap = 0;
     cudaMemPool_t pool = nullptr;  // graphs and temporaries (keeps up to 4 GiB cached between calls)
+    std::unordered_map<std::string, std::unique_ptr<BatchPlan>> plans;  // khz_count's prepared launches
     std::mutex mu;
+};
+
+struct khz_batch {
+    khz_ctx *ctx;
+    std::unique_ptr<BatchPlan> plan;
 };
 
 namespace {
@@ -143,29 +173,6 @@ khz_graph add_graph(khz_ctx *ctx, const Graph &g) {
     return (khz_graph)ctx->graphs.size();
 }
 
-khz_status ensure_rows(khz_ctx *ctx, size_t rows) {
-    if (ctx->rows_cap >= rows) return KHZ_OK;
-    if (ctx->d_rows) cudaFree(ctx->d_rows);
-    if (ctx->d_mult) cudaFree(ctx->d_mult);
-    if (ctx->d_extadd) cudaFree(ctx->d_extadd);
-    ctx->d_rows = nullptr;
-    ctx->d_mult = nullptr;
-    ctx->d_extadd = nullptr;
-    ctx->rows_cap = 0;
-    KHZ_CUDA(cudaMalloc(&ctx->d_rows, sizeof(uint64_t) * kRow * rows * 2));
-    KHZ_CUDA(cudaMalloc(&ctx->d_mult, sizeof(uint32_t) * KHZ_MAX_COUNTS * rows));
-    KHZ_CUDA(cudaMalloc(&ctx->d_extadd, sizeof(uint64_t) * rows));
-    ctx->rows_cap = rows;
-    return KHZ_OK;
-}
-
-khz_status ensure_counters(Workspace *ws) {
-    if (ws->counters) return KHZ_OK;
-    KHZ_CUDA(cudaMalloc(&ws->counters, 4096));
-    ws->counters_bytes = 4096;
-    return KHZ_OK;
-}
-
 // oriented view of g (g itself when oriented; else a cached orientation)
 khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
     Graph *g = get_graph(ctx, h);
@@ -180,190 +187,210 @@ khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
         khz_status st = orient_graph(*g, &o, s);
         if (st) return st;
         khz_graph oh = add_graph(ctx, o);
-        g = get_graph(ctx, h);  // vector may have moved
+        g = get_graph(ctx, h);  // the table may have moved
         g->oriented_view = oh;
     }
     *out = get_graph(ctx, g->oriented_view);
     return KHZ_OK;
 }
 
-struct Enq {
-    uint32_t launches = 0;
-    uint32_t engine = 0;
-    LaunchStats ls;  // per-phase events / bytes (timed calls only)
-};
-
-// Enqueue one (graph, app) count into raw row `row` (zeroed by the caller); returns the host-side
-// NumExtensions addend (one depth-0 embedding per start vertex per run).
-khz_status enqueue_count(khz_ctx *ctx, khz_graph h, int app, size_t row, std::vector<DfsJob> *dfs_jobs,
-                         std::vector<Plan> *dfs_plans, uint64_t *ext_add, uint32_t *slot_cap, Enq *enq,
-                         cudaStream_t s, bool batched) {
-    const AppDef &def = app_def(app);
-    Graph *g = get_graph(ctx, h);
-    if (!g) return KHZ_ERR_ARG;
-    const bool stats = ctx->cfg.want_algo_bytes != 0;
-    int engine = ctx->cfg.engine;
+// engine for one job under the context's configuration: the bitmap engine for clique apps on
+// graphs that are a DAG in id order or symmetric (oriented once, cached); the DFS engine otherwise
+int pick_engine(const khz_config &cfg, const AppDef &def, const Graph &g) {
+    int engine = cfg.engine;
     if (engine == KHZ_ENGINE_AUTO) engine = def.clique ? KHZ_ENGINE_BITMAP : KHZ_ENGINE_DFS;
     if (engine == KHZ_ENGINE_BITMAP && !def.clique) engine = KHZ_ENGINE_DFS;
-    uint64_t *raw = ctx->d_rows + row * kRow;
-    // the bitmap engine needs a DAG in id order; a symmetric graph is oriented first (cached);
-    // any other shape runs the schedule as stored, like the reference does
-    if (engine == KHZ_ENGINE_BITMAP && !g->oriented && !g->symmetric) engine = KHZ_ENGINE_DFS;
-    if (engine == KHZ_ENGINE_BITMAP && !batched) {
-        Graph *og = nullptr;
-        khz_status st = oriented_of(ctx, h, &og, s);
-        if (st) return st;
-        uint32_t overflow = 0;
-        const uint32_t before = enq->ls.launches;
-        st = bitmap_clique_run(*og, def.clique_k, stats, ctx->cfg.bitmap_warp_max, ctx->cfg.bitmap_block_warps,
-                               raw, &ctx->ws, s, &enq->ls, &overflow);
-        if (st) return st;
-        enq->launches += enq->ls.launches - before;
-        if (overflow > 0) {
-            DfsJob j{};
-            j.off = og->off;
-            j.adj = og->adj;
-            j.n = og->n;
-            j.num_units = og->m;
-            j.out_base = (uint32_t)row;
-            j.min_deg = bitmap_block_max_degree() + 1;
-            j.plan_idx = (uint32_t)dfs_plans->size();
-            dfs_plans->push_back(def.plans[0]);
-            dfs_jobs->push_back(j);
-            *slot_cap = std::max(*slot_cap, og->max_degree);
-        }
-        *ext_add = og->n;
-        enq->engine = KHZ_ENGINE_BITMAP;
-        return KHZ_OK;
-    }
-    // DFS engine on the graph as stored (oriented graphs use the oriented lists)
-    for (int r = 0; r < def.num_runs; ++r) {
-        DfsJob j{};
-        j.off = g->off;
-        j.adj = g->adj;
-        j.n = g->n;
-        j.num_units = g->m;
-        j.out_base = (uint32_t)row;
-        j.min_deg = 0;
-        j.plan_idx = (uint32_t)dfs_plans->size();
-        dfs_plans->push_back(def.plans[r]);
-        dfs_jobs->push_back(j);
-    }
-    *slot_cap = std::max(*slot_cap, g->max_degree);
-    *ext_add = (uint64_t)g->n * def.num_runs;
-    enq->engine = KHZ_ENGINE_DFS;
-    return KHZ_OK;
+    if (engine == KHZ_ENGINE_BITMAP && !g.oriented && !g.symmetric) engine = KHZ_ENGINE_DFS;
+    return engine;
 }
 
-khz_status run_dfs(khz_ctx *ctx, std::vector<DfsJob> &jobs, std::vector<Plan> &plans, uint32_t slot_cap,
-                   Enq *enq, cudaStream_t s) {
-    if (jobs.empty()) return KHZ_OK;
-    uint64_t begin = 0;
-    for (auto &j : jobs) {
-        j.unit_begin = begin;
-        begin += j.num_units;
+khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, std::unique_ptr<BatchPlan> *out) {
+    if (n <= 0) {
+        set_error("empty batch");
+        return KHZ_ERR_ARG;
     }
-    const uint32_t before = enq->ls.launches;
-    khz_status st = dfs_run(jobs.data(), (int)jobs.size(), plans.data(), (int)plans.size(), slot_cap,
-                            ctx->cfg.want_algo_bytes != 0, ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk,
-                            ctx->d_rows, &ctx->ws, s, &enq->ls);
-    enq->launches += enq->ls.launches - before;
-    return st;
-}
-
-khz_status finalize(khz_ctx *ctx, const std::vector<int> &apps, const std::vector<uint64_t> &ext_add,
-                    uint64_t *d_final, cudaStream_t s) {
-    const size_t rows = apps.size();
-    std::vector<uint32_t> mult(rows * KHZ_MAX_COUNTS, 1);
-    for (size_t r = 0; r < rows; ++r) {
-        const AppDef &d = app_def(apps[r]);
-        for (int c = 0; c < KHZ_MAX_COUNTS; ++c) mult[r * KHZ_MAX_COUNTS + c] = c < d.num_counts ? d.mult[c] : 1;
-    }
-    KHZ_CUDA(cudaMemcpyAsync(ctx->d_mult, mult.data(), sizeof(uint32_t) * mult.size(), cudaMemcpyHostToDevice, s));
-    KHZ_CUDA(cudaMemcpyAsync(ctx->d_extadd, ext_add.data(), sizeof(uint64_t) * rows, cudaMemcpyHostToDevice, s));
-    finalize_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(ctx->d_rows, (int)rows, ctx->d_mult,
-                                                                   ctx->d_extadd, d_final, ctx->d_bad);
-    KHZ_CUDA(cudaGetLastError());
-    return KHZ_OK;
-}
-
-khz_status count_many(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64_t *d_final, cudaStream_t s,
-                      Enq *enq, bool timed, double *ms) {
-    for (int i = 0; i < n_jobs; ++i) {
+    for (int i = 0; i < n; ++i) {
         if (jobs[i].app < 0 || jobs[i].app >= KHZ_NUM_APPS) {
             set_error("invalid app id %d", jobs[i].app);
             return KHZ_ERR_ARG;
         }
         if (!get_graph(ctx, jobs[i].graph)) return KHZ_ERR_ARG;
     }
-    khz_status st = ensure_rows(ctx, (size_t)n_jobs);
-    if (st) return st;
-    st = ensure_counters(&ctx->ws);
-    if (st) return st;
-    if (!ctx->d_bad) KHZ_CUDA(cudaMalloc(&ctx->d_bad, sizeof(unsigned int)));
-    KHZ_CUDA(cudaMemsetAsync(ctx->d_bad, 0, sizeof(unsigned int), s));
-    KHZ_CUDA(cudaMemsetAsync(ctx->d_rows, 0, sizeof(uint64_t) * kRow * n_jobs, s));
-    // orientations are prepared before the timed region
-    const bool batched = n_jobs > 1;
-    if (!batched) {
-        const AppDef &def = app_def(jobs[0].app);
-        int engine = ctx->cfg.engine;
-        Graph *g0 = get_graph(ctx, jobs[0].graph);
-        if ((engine == KHZ_ENGINE_AUTO || engine == KHZ_ENGINE_BITMAP) && def.clique && !g0->oriented &&
-            g0->symmetric) {
-            Graph *og;
-            st = oriented_of(ctx, jobs[0].graph, &og, s);
-            if (st) return st;
-        }
-    }
-    uint64_t *d_phase_bytes = ctx->ws.counters + 16;
-    KHZ_CUDA(cudaMemsetAsync(d_phase_bytes, 0, sizeof(uint64_t) * kPhases, s));
-    if (timed) {
-        enq->ls.ev_begin = ctx->ph_begin;
-        enq->ls.ev_end = ctx->ph_end;
-        enq->ls.d_phase_bytes = d_phase_bytes;
-    }
-    if (timed) KHZ_CUDA(cudaEventRecord(ctx->ev0, s));
+    auto P = std::make_unique<BatchPlan>();
+    P->rows = n;
+    P->stats = ctx->cfg.want_algo_bytes != 0;
+    std::vector<BJob> bjobs;
     std::vector<DfsJob> djobs;
     std::vector<Plan> plans;
-    std::vector<uint64_t> ext_add(n_jobs, 0);
-    std::vector<int> apps(n_jobs);
-    uint32_t slot_cap = 32;
-    for (int i = 0; i < n_jobs; ++i) {
-        apps[i] = jobs[i].app;
-        st = enqueue_count(ctx, jobs[i].graph, jobs[i].app, (size_t)i, &djobs, &plans, &ext_add[i], &slot_cap, enq,
-                           s, batched);
-        if (st) return st;
+    std::vector<uint64_t> ext_add(n, 0);
+    std::vector<uint32_t> mult((size_t)n * KHZ_MAX_COUNTS, 1);
+    uint32_t bmax = 0, slot_cap = 32;
+    uint64_t vbase = 0, bm_entries = 0, unit_base = 0;
+    auto add_dfs = [&](const Graph &g, const Plan &pl, int row, uint32_t min_deg) {
+        DfsJob j{};
+        j.off = g.off;
+        j.adj = g.adj;
+        j.n = g.n;
+        j.plan_idx = (uint32_t)plans.size();
+        j.unit_begin = unit_base;
+        j.num_units = g.m;
+        j.out_base = (uint32_t)row;
+        j.min_deg = min_deg;
+        plans.push_back(pl);
+        djobs.push_back(j);
+        unit_base += g.m;
+        slot_cap = std::max(slot_cap, g.max_degree);
+    };
+    for (int i = 0; i < n; ++i) {
+        const AppDef &def = app_def(jobs[i].app);
+        P->apps.push_back(jobs[i].app);
+        for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
+        const int engine = pick_engine(ctx->cfg, def, *get_graph(ctx, jobs[i].graph));
+        if (engine == KHZ_ENGINE_BITMAP) {
+            Graph *og = nullptr;
+            khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
+            if (st) return st;
+            BJob b{og->off, og->adj, og->n, def.clique_k, vbase, (uint32_t)i, 0};
+            bjobs.push_back(b);
+            vbase += og->n;
+            bm_entries += og->m;
+            bmax = std::max(bmax, og->max_degree);
+            if (og->max_degree > bitmap_block_max_degree())
+                add_dfs(*og, def.plans[0], i, bitmap_block_max_degree() + 1);
+            ext_add[i] = og->n;
+            P->engine = KHZ_ENGINE_BITMAP;
+        } else {
+            const Graph &g = *get_graph(ctx, jobs[i].graph);
+            for (int r = 0; r < def.num_runs; ++r) add_dfs(g, def.plans[r], i, 0);
+            ext_add[i] = (uint64_t)g.n * def.num_runs;
+        }
     }
-    st = run_dfs(ctx, djobs, plans, slot_cap, enq, s);
+    P->has_bitmap = !bjobs.empty();
+    P->has_dfs = !djobs.empty();
+    const uint64_t list_cap = std::min<uint64_t>(std::max<uint64_t>(vbase, 1), bm_entries / 65 + 1);
+    const uint64_t dfs_warps = dfs_total_warps(ctx->cfg.dfs_warps_per_sm);
+    size_t bytes = 2 * Arena::round(sizeof(uint64_t) * kRowWords * n) + Arena::round(sizeof(uint32_t) * mult.size()) +
+                   Arena::round(sizeof(uint64_t) * n) + Arena::round(sizeof(unsigned int)) +
+                   Arena::round(sizeof(uint64_t) * kPhases);
+    if (P->has_bitmap) bytes += bitmap_arena_bytes((int)bjobs.size(), list_cap);
+    if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap);
+    cudaError_t e = cudaMalloc(&P->mem, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        P->mem = nullptr;
+        set_error("counting launch needs %llu bytes of device scratch: %s", (unsigned long long)bytes,
+                  cudaGetErrorString(e));
+        return KHZ_ERR_OOM;
+    }
+    P->arena.base = (char *)P->mem;
+    P->arena.cap = bytes;
+    P->d_raw = P->arena.take<uint64_t>((size_t)kRowWords * n);
+    P->d_final = P->arena.take<uint64_t>((size_t)kRowWords * n);
+    P->d_mult = P->arena.take<uint32_t>(mult.size());
+    P->d_extadd = P->arena.take<uint64_t>(n);
+    P->d_bad = P->arena.take<unsigned int>(1);
+    P->d_phase_bytes = P->arena.take<uint64_t>(kPhases);
+    KHZ_CUDA(cudaMemcpyAsync(P->d_mult, mult.data(), sizeof(uint32_t) * mult.size(), cudaMemcpyHostToDevice, s));
+    KHZ_CUDA(cudaMemcpyAsync(P->d_extadd, ext_add.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
+    khz_status st = KHZ_OK;
+    if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, &P->arena, &P->bl, s);
     if (st) return st;
-    if (timed) KHZ_CUDA(cudaEventRecord(ctx->ev1, s));
-    st = finalize(ctx, apps, ext_add, d_final, s);
+    if (P->has_dfs)
+        st = dfs_prepare(djobs, plans, slot_cap, ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, P->stats, &P->arena,
+                         &P->dl, s);
     if (st) return st;
-    enq->launches += 1;
-    if (timed) {
-        KHZ_CUDA(cudaEventSynchronize(ctx->ev1));
-        float f = 0;
-        KHZ_CUDA(cudaEventElapsedTime(&f, ctx->ev0, ctx->ev1));
-        *ms = f;
+    if (cudaMallocHost(&P->h_final, sizeof(uint64_t) * ((size_t)kRowWords * n + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        P->h_final = nullptr;
+        set_error("pinned result buffer allocation failed");
+        return KHZ_ERR_OOM;
+    }
+    KHZ_CUDA(cudaStreamSynchronize(s));
+    *out = std::move(P);
+    return KHZ_OK;
+}
+
+// Enqueue the plan: zero the counters, the engines' launches, finalize.  `ls` (may be null)
+// records per-phase events; ev_begin / ev_end (may be null) bracket the counting launches.
+khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
+    KHZ_CUDA(cudaMemsetAsync(P->d_raw, 0, sizeof(uint64_t) * kRowWords * P->rows, s));
+    KHZ_CUDA(cudaMemsetAsync(P->d_bad, 0, sizeof(unsigned int), s));
+    KHZ_CUDA(cudaMemsetAsync(P->d_phase_bytes, 0, sizeof(uint64_t) * kPhases, s));
+    if (ls) ls->d_phase_bytes = P->d_phase_bytes;
+    if (ev_begin) KHZ_CUDA(cudaEventRecord(ev_begin, s));
+    khz_status st = KHZ_OK;
+    if (P->has_bitmap) st = bitmap_enqueue(P->bl, P->d_raw, s, ls);
+    if (st) return st;
+    if (P->has_dfs) st = dfs_enqueue(P->dl, P->d_raw, s, ls);
+    if (st) return st;
+    if (ev_end) KHZ_CUDA(cudaEventRecord(ev_end, s));
+    finalize_kernel<<<(unsigned)((P->rows + 127) / 128), 128, 0, s>>>(P->d_raw, P->rows, P->d_mult, P->d_extadd,
+                                                                      P->d_final, P->d_bad);
+    KHZ_CUDA(cudaGetLastError());
+    if (ls) ls->launches += 1;
+    return KHZ_OK;
+}
+
+// copy the finalized rows to the plan's pinned buffer and wait for them
+khz_status read_plan(BatchPlan *P, cudaStream_t s) {
+    const size_t words = (size_t)kRowWords * P->rows;
+    KHZ_CUDA(cudaMemcpyAsync(P->h_final, P->d_final, sizeof(uint64_t) * words, cudaMemcpyDeviceToHost, s));
+    KHZ_CUDA(cudaMemcpyAsync(P->h_final + words, P->d_bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    KHZ_CUDA(cudaStreamSynchronize(s));
+    if (*(const unsigned int *)(P->h_final + words)) {
+        set_error("raw count not divisible by the pattern multiplicity (input is not an undirected graph)");
+        return KHZ_ERR_MULTIPLICITY;
     }
     return KHZ_OK;
 }
 
-khz_status fill_phases(khz_ctx *ctx, const Enq &enq, khz_stats *stats, cudaStream_t s) {
+khz_status fill_stats(khz_ctx *ctx, BatchPlan *P, const LaunchStats &ls, bool timed, khz_stats *stats) {
+    uint64_t ext = 0, bytes = 0;
+    for (int r = 0; r < P->rows; ++r) {
+        ext += P->h_final[(size_t)r * kRowWords + KHZ_MAX_COUNTS];
+        bytes += P->h_final[(size_t)r * kRowWords + KHZ_MAX_COUNTS + 1];
+    }
+    stats->num_extensions = ext;
+    stats->algo_bytes = bytes;
+    stats->engine = P->engine;
+    stats->launches = ls.launches;
+    stats->kernel_ms = 0;
     uint64_t pb[kPhases] = {0, 0, 0, 0};
-    KHZ_CUDA(cudaMemcpyAsync(pb, ctx->ws.counters + 16, sizeof(pb), cudaMemcpyDeviceToHost, s));
-    KHZ_CUDA(cudaStreamSynchronize(s));
+    KHZ_CUDA(cudaMemcpy(pb, P->d_phase_bytes, sizeof(pb), cudaMemcpyDeviceToHost));
     for (int p = 0; p < kPhases; ++p) {
         stats->phase_ms[p] = 0;
         stats->phase_bytes[p] = pb[p];
-        stats->phase_launches[p] = enq.ls.phase_launches[p];
-        if (enq.ls.used[p]) {
+        stats->phase_launches[p] = ls.phase_launches[p];
+        if (timed && ls.used[p]) {
             float f = 0;
             KHZ_CUDA(cudaEventElapsedTime(&f, ctx->ph_begin[p], ctx->ph_end[p]));
             stats->phase_ms[p] = f;
         }
     }
+    if (timed) {
+        float f = 0;
+        KHZ_CUDA(cudaEventElapsedTime(&f, ctx->ev0, ctx->ev1));
+        stats->kernel_ms = f;
+    }
+    return KHZ_OK;
+}
+
+// the cached prepared launch of one (graph, app) under the current configuration
+khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, BatchPlan **out) {
+    char key[160];
+    snprintf(key, sizeof(key), "%u/%d/%d/%d/%d/%d", g, app, ctx->cfg.engine, ctx->cfg.want_algo_bytes,
+             ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk);
+    auto it = ctx->plans.find(key);
+    if (it != ctx->plans.end()) {
+        *out = it->second.get();
+        return KHZ_OK;
+    }
+    khz_job j{g, (int32_t)app, 0};
+    std::unique_ptr<BatchPlan> P;
+    khz_status st = build_plan(ctx, &j, 1, s, &P);
+    if (st) return st;
+    *out = P.get();
+    ctx->plans[key] = std::move(P);
     return KHZ_OK;
 }
 
@@ -431,14 +458,8 @@ khz_status khz_ctx_destroy(khz_ctx *ctx) {
             if (ctx->live[i]) free_graph_memory(&ctx->graphs[i]);
     }
     cudaDeviceSynchronize();
+    ctx->plans.clear();
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
-    if (ctx->ws.slots) cudaFree(ctx->ws.slots);
-    if (ctx->ws.counters) cudaFree(ctx->ws.counters);
-    if (ctx->ws.tmp) cudaFree(ctx->ws.tmp);
-    if (ctx->d_rows) cudaFree(ctx->d_rows);
-    if (ctx->d_mult) cudaFree(ctx->d_mult);
-    if (ctx->d_extadd) cudaFree(ctx->d_extadd);
-    if (ctx->d_bad) cudaFree(ctx->d_bad);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (int p = 0; p < kPhases; ++p) {
@@ -458,6 +479,7 @@ khz_status khz_ctx_set_config(khz_ctx *ctx, const khz_config *cfg) {
         set_error("invalid engine %d", cfg->engine);
         return KHZ_ERR_ARG;
     }
+    std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cfg = *cfg;
     if (ctx->cfg.dfs_warps_per_sm <= 0) ctx->cfg.dfs_warps_per_sm = 16;
     if (ctx->cfg.dfs_chunk <= 0) ctx->cfg.dfs_chunk = 8;
@@ -690,6 +712,7 @@ khz_status khz_graph_free(khz_ctx *ctx, khz_graph h) {
     if (!g) return KHZ_ERR_ARG;
     // work on any stream may still read the graph: order the release after all of it
     KHZ_CUDA(cudaDeviceSynchronize());
+    ctx->plans.clear();  // prepared launches hold the graph's device pointers
     AllocScope scope(ctx->pool, nullptr);
     const khz_graph ov = g->oriented_view;
     free_graph_memory(g);
@@ -724,10 +747,14 @@ khz_status khz_count_async(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *
         return KHZ_ERR_ARG;
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
-    khz_job j{g, (int32_t)app, 0};
-    Enq enq;
-    double ms = 0;
-    return count_many(ctx, &j, 1, d_out, (cudaStream_t)stream, &enq, false, &ms);
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchPlan *P = nullptr;
+    st = cached_plan(ctx, g, app, s, &P);
+    if (st) return st;
+    st = enqueue_plan(P, s, nullptr, nullptr, nullptr);
+    if (st) return st;
+    KHZ_CUDA(cudaMemcpyAsync(d_out, P->d_final, sizeof(uint64_t) * kRowWords, cudaMemcpyDeviceToDevice, s));
+    return KHZ_OK;
 }
 
 khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts, khz_stats *stats, void *stream) {
@@ -739,34 +766,19 @@ khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
-    khz_job j{g, (int32_t)app, 0};
-    Enq enq;
-    double ms = 0;
-    st = ensure_rows(ctx, 1);
+    BatchPlan *P = nullptr;
+    st = cached_plan(ctx, g, app, s, &P);
     if (st) return st;
-    uint64_t *d_final = ctx->d_rows + ctx->rows_cap * kRow;
-    st = count_many(ctx, &j, 1, d_final, s, &enq, true, &ms);
+    LaunchStats ls;
+    ls.ev_begin = ctx->ph_begin;
+    ls.ev_end = ctx->ph_end;
+    st = enqueue_plan(P, s, &ls, ctx->ev0, ctx->ev1);
     if (st) return st;
-    uint64_t row[kRow];
-    unsigned int bad = 0;
-    KHZ_CUDA(cudaMemcpyAsync(row, d_final, sizeof(row), cudaMemcpyDeviceToHost, s));
-    KHZ_CUDA(cudaMemcpyAsync(&bad, ctx->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
-    KHZ_CUDA(cudaStreamSynchronize(s));
-    if (bad) {
-        set_error("raw count not divisible by the pattern multiplicity (input is not an undirected graph)");
-        return KHZ_ERR_MULTIPLICITY;
-    }
+    st = read_plan(P, s);
+    if (st) return st;
     const int nc = app_def(app).num_counts;
-    for (int c = 0; c < nc; ++c) counts[c] = row[c];
-    if (stats) {
-        stats->num_extensions = row[KHZ_MAX_COUNTS];
-        stats->algo_bytes = row[KHZ_MAX_COUNTS + 1];
-        stats->kernel_ms = ms;
-        stats->engine = enq.engine;
-        stats->launches = enq.launches;
-        st = fill_phases(ctx, enq, stats, s);
-        if (st) return st;
-    }
+    for (int c = 0; c < nc; ++c) counts[c] = P->h_final[c];
+    if (stats) return fill_stats(ctx, P, ls, true, stats);
     return KHZ_OK;
 }
 
@@ -780,40 +792,93 @@ khz_status khz_count_batch(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
-    st = ensure_rows(ctx, (size_t)n_jobs);
+    std::unique_ptr<BatchPlan> P;
+    st = build_plan(ctx, jobs, n_jobs, s, &P);
     if (st) return st;
-    uint64_t *d_final = ctx->d_rows + ctx->rows_cap * kRow;
-    Enq enq;
-    double ms = 0;
-    st = count_many(ctx, jobs, n_jobs, d_final, s, &enq, true, &ms);
+    LaunchStats ls;
+    ls.ev_begin = ctx->ph_begin;
+    ls.ev_end = ctx->ph_end;
+    st = enqueue_plan(P.get(), s, &ls, ctx->ev0, ctx->ev1);
     if (st) return st;
-    std::vector<uint64_t> rows((size_t)n_jobs * kRow);
-    unsigned int bad = 0;
-    KHZ_CUDA(cudaMemcpyAsync(rows.data(), d_final, sizeof(uint64_t) * rows.size(), cudaMemcpyDeviceToHost, s));
-    KHZ_CUDA(cudaMemcpyAsync(&bad, ctx->d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s));
-    KHZ_CUDA(cudaStreamSynchronize(s));
-    if (bad) {
-        set_error("raw count not divisible by the pattern multiplicity (input is not an undirected graph)");
-        return KHZ_ERR_MULTIPLICITY;
-    }
+    st = read_plan(P.get(), s);
+    if (st) return st;
     for (int i = 0; i < n_jobs; ++i) {
-        for (int c = 0; c < KHZ_MAX_COUNTS; ++c) counts[(size_t)i * KHZ_MAX_COUNTS + c] = rows[(size_t)i * kRow + c];
-        if (num_ext) num_ext[i] = rows[(size_t)i * kRow + KHZ_MAX_COUNTS];
+        for (int c = 0; c < KHZ_MAX_COUNTS; ++c)
+            counts[(size_t)i * KHZ_MAX_COUNTS + c] = P->h_final[(size_t)i * kRowWords + c];
+        if (num_ext) num_ext[i] = P->h_final[(size_t)i * kRowWords + KHZ_MAX_COUNTS];
     }
-    if (stats) {
-        uint64_t ext = 0, bytes = 0;
-        for (int i = 0; i < n_jobs; ++i) {
-            ext += rows[(size_t)i * kRow + KHZ_MAX_COUNTS];
-            bytes += rows[(size_t)i * kRow + KHZ_MAX_COUNTS + 1];
+    if (stats) return fill_stats(ctx, P.get(), ls, true, stats);
+    return KHZ_OK;
+}
+
+khz_status khz_batch_create(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint32_t flags, khz_batch **out,
+                            void *stream) {
+    khz_status st = check_ctx(ctx);
+    if (st) return st;
+    if (!out || !jobs || n_jobs <= 0) {
+        set_error("empty batch or null argument");
+        return KHZ_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t s = (cudaStream_t)stream;
+    std::unique_ptr<khz_batch> b(new khz_batch{ctx, nullptr});
+    st = build_plan(ctx, jobs, n_jobs, s, &b->plan);
+    if (st) return st;
+    if (flags & KHZ_BATCH_CUDA_GRAPH) {
+        cudaStream_t cs = nullptr;
+        KHZ_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            st = enqueue_plan(b->plan.get(), cs, nullptr, nullptr, nullptr);
+            e = cudaStreamEndCapture(cs, &b->plan->graph);
         }
-        stats->num_extensions = ext;
-        stats->algo_bytes = bytes;
-        stats->kernel_ms = ms;
-        stats->engine = KHZ_ENGINE_DFS;
-        stats->launches = enq.launches;
-        st = fill_phases(ctx, enq, stats, s);
+        if (e == cudaSuccess && st == KHZ_OK) e = cudaGraphInstantiate(&b->plan->exec, b->plan->graph, 0);
+        cudaStreamDestroy(cs);
         if (st) return st;
+        if (e != cudaSuccess) return cuda_fail(e, "capturing the batch into a CUDA graph");
     }
+    *out = b.release();
+    return KHZ_OK;
+}
+
+khz_status khz_batch_launch(khz_batch *b, void *stream) {
+    if (!b) {
+        set_error("null batch");
+        return KHZ_ERR_ARG;
+    }
+    khz_status st = check_ctx(b->ctx);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->plan->exec) {
+        KHZ_CUDA(cudaGraphLaunch(b->plan->exec, s));
+        return KHZ_OK;
+    }
+    return enqueue_plan(b->plan.get(), s, nullptr, nullptr, nullptr);
+}
+
+khz_status khz_batch_wait(khz_batch *b, uint64_t *counts, uint64_t *num_ext, void *stream) {
+    if (!b || !counts) {
+        set_error("null argument");
+        return KHZ_ERR_ARG;
+    }
+    khz_status st = check_ctx(b->ctx);
+    if (st) return st;
+    BatchPlan *P = b->plan.get();
+    st = read_plan(P, (cudaStream_t)stream);
+    if (st) return st;
+    for (int i = 0; i < P->rows; ++i) {
+        for (int c = 0; c < KHZ_MAX_COUNTS; ++c)
+            counts[(size_t)i * KHZ_MAX_COUNTS + c] = P->h_final[(size_t)i * kRowWords + c];
+        if (num_ext) num_ext[i] = P->h_final[(size_t)i * kRowWords + KHZ_MAX_COUNTS];
+    }
+    return KHZ_OK;
+}
+
+khz_status khz_batch_destroy(khz_batch *b) {
+    if (!b) return KHZ_OK;
+    cudaSetDevice(b->ctx->device);
+    cudaDeviceSynchronize();
+    delete b;
     return KHZ_OK;
 }
 

@@ -3,7 +3,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
+#include <vector>
 
 #include "khz.h"
 
@@ -95,17 +97,64 @@ struct DfsJob {
     uint32_t min_deg;      // skip start vertices whose degree is below this (handled elsewhere)
 };
 
-// Workspace: per-launch device scratch owned by a context
-struct Workspace {
-    uint32_t *slots = nullptr;   // dfs warps * kNumSlots * slot_cap
-    uint64_t slot_bytes = 0;
-    uint64_t *counters = nullptr;  // small device scratch: queue heads, stats
-    uint64_t counters_bytes = 0;
-    void *tmp = nullptr;          // cub temp / lists
-    uint64_t tmp_bytes = 0;
-    uint64_t *pinned = nullptr;   // host pinned mirror for results
-    uint64_t pinned_bytes = 0;
+constexpr int kRowWords = KHZ_MAX_COUNTS + 2;  // counter row: counts[6], NumExtensions, algorithmic bytes
+
+// one (oriented graph, clique app) job of a bitmap-engine launch; jobs are sorted by vbase and
+// their start vertices form one global index space [0, sum n)
+struct BJob {
+    const uint64_t *off;
+    const uint32_t *adj;
+    uint32_t n;
+    int32_t k;          // clique size 3, 4 or 5
+    uint64_t vbase;
+    uint32_t out_row;
+    uint32_t pad;
 };
+
+// bump allocator over one device allocation
+struct Arena {
+    char *base = nullptr;
+    size_t used = 0, cap = 0;
+    static size_t round(size_t b) { return (b + 255) & ~(size_t)255; }
+    template <typename T>
+    T *take(size_t count) {
+        const size_t b = round(sizeof(T) * std::max<size_t>(count, 1));
+        if (used + b > cap) return nullptr;
+        T *p = (T *)(base + used);
+        used += b;
+        return p;
+    }
+};
+
+// device resources and launch shapes of one bitmap-engine launch sequence
+struct BitmapLaunch {
+    const BJob *d_jobs = nullptr;
+    int n_jobs = 0;
+    uint64_t n_total = 0;
+    uint32_t *mid_list = nullptr, *large_list = nullptr;
+    unsigned int *cnt = nullptr;
+    unsigned long long *queues = nullptr;
+    int large_dcap = 0;
+    bool has_mid = false, has_large = false, stats = false;
+    int sms = 0;
+    size_t block_smem[2] = {0, 0};
+    int block_threads[2] = {0, 0}, block_grid[2] = {0, 0}, block_dcap[2] = {0, 0};
+};
+
+// device resources and launch shape of one DFS-engine launch
+struct DfsLaunch {
+    const DfsJob *d_jobs = nullptr;
+    int n_jobs = 0;
+    const Plan *d_plans = nullptr;
+    uint64_t total_units = 0;
+    uint32_t *slots = nullptr;
+    uint32_t slot_cap = 0;
+    int blocks = 0, threads = 0;
+    uint32_t chunk = 8;
+    unsigned long long *queue = nullptr;
+    bool stats = false;
+};
+
 
 // Device allocation for graphs and temporaries: from the context's stream-ordered pool when an
 // AllocScope is active on this thread (cudaMallocFromPoolAsync / cudaFreeAsync on its stream),
@@ -147,19 +196,24 @@ struct LaunchStats {
     uint32_t phase_launches[kPhases] = {0, 0, 0, 0};
     uint64_t *d_phase_bytes = nullptr;  // device [kPhases], instrumented runs add per-phase bytes
 };
-// DFS engine: runs jobs; d_out rows of (KHZ_MAX_COUNTS + 2) uint64 must be zeroed by the caller.
-khz_status dfs_run(const DfsJob *h_jobs, int n_jobs, const Plan *h_plans, int n_plans, uint32_t slot_cap,
-                   bool stats, int warps_per_sm, int chunk, uint64_t *d_out, Workspace *ws, cudaStream_t s,
-                   LaunchStats *ls);
+// DFS engine.  Jobs carry unit_begin (prefix of num_units); rows of kRowWords uint64 must be
+// zeroed by the caller.  No host synchronisation in dfs_enqueue.
+uint64_t dfs_total_warps(int warps_per_sm);
+size_t dfs_arena_bytes(int n_jobs, int n_plans, uint64_t total_warps, uint32_t slot_cap);
+khz_status dfs_prepare(const std::vector<DfsJob> &jobs, const std::vector<Plan> &plans, uint32_t slot_cap,
+                       int warps_per_sm, int chunk, bool stats, Arena *arena, DfsLaunch *dl, cudaStream_t s);
+khz_status dfs_enqueue(const DfsLaunch &dl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_plans, uint64_t total_units,
                                uint32_t chunk, uint32_t *slots, uint32_t slot_cap, unsigned long long *queue,
                                uint64_t *d_raw, int blocks, int threads, cudaStream_t s);
-// Bitmap clique engine on an oriented graph: adds count / NumExtensions-without-n-and-m / bytes into
-// d_out[0], d_out[6], d_out[7].  Vertices whose out-degree exceeds the block tier are returned in
-// *overflow (device list) for the DFS engine.
-khz_status bitmap_clique_run(const Graph &g, int k, bool stats, int warp_max, int block_warps,
-                             uint64_t *d_out, Workspace *ws, cudaStream_t s, LaunchStats *ls,
-                             uint32_t *n_overflow);
+// Bitmap clique engine over oriented graphs.  Adds each job's count (row[0]), its NumExtensions
+// beyond depth 0 (row[6]) and, instrumented, the algorithmic bytes (row[7]).  Start vertices of
+// out-degree above bitmap_block_max_degree() are skipped: run them on the DFS engine with
+// DfsJob::min_deg.  No host synchronisation in bitmap_enqueue.
+size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap);
+khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
+                          Arena *arena, BitmapLaunch *bl, cudaStream_t s);
+khz_status bitmap_enqueue(const BitmapLaunch &bl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 uint32_t bitmap_block_max_degree();
 
 }  // namespace khz

@@ -44,7 +44,8 @@ EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_g
            "khz_last_error_string", "khz_abi_version", "khz_graph_from_edges", "khz_graph_load_dgraph",
            "khz_graph_orient", "khz_graph_generate_rmat", "khz_graph_info_get", "khz_graph_export_csr",
            "khz_graph_write_dgraph", "khz_graph_free", "khz_count", "khz_count_async", "khz_app_num_counts",
-           "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch", "khz_count_noalloc"]
+           "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch", "khz_count_noalloc",
+           "khz_batch_create", "khz_batch_launch", "khz_batch_wait", "khz_batch_destroy"]
 
 
 class KhzError(RuntimeError):
@@ -121,6 +122,10 @@ def lib():
             "khz_count_batch": (i32, [vp, P(Job), i32, P(u64), P(u64), P(Stats), vp]),
             "khz_set_op_batch": (i32, [i32, vp, vp, vp, vp, vp, vp, vp, u32, vp]),
             "khz_count_noalloc": (i32, [vp, vp, u32, u64, i32, vp, vp]),
+            "khz_batch_create": (i32, [vp, P(Job), i32, u32, P(vp), vp]),
+            "khz_batch_launch": (i32, [vp, vp]),
+            "khz_batch_wait": (i32, [vp, P(u64), P(u64), vp]),
+            "khz_batch_destroy": (i32, [vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -269,6 +274,37 @@ class Context:
             nc = num_counts(app)
             out.append([int(counts[i * MAX_COUNTS + c]) for c in range(nc)])
         return out, [int(x) for x in ext], st
+
+
+class Batch:
+    """A prepared batch of (graph, app) jobs: one launch sequence for all of them, optionally
+    captured into a CUDA graph (cuda_graph=True) and replayed by launch()."""
+
+    def __init__(self, ctx, jobs, cuda_graph=False, stream=None):
+        self.jobs = list(jobs)
+        arr = (Job * len(self.jobs))()
+        for i, (g, app) in enumerate(self.jobs):
+            arr[i].graph = g.handle
+            arr[i].app = _app_id(app)
+        p = ctypes.c_void_p()
+        _check(lib().khz_batch_create(ctx.ptr, arr, len(self.jobs), 1 if cuda_graph else 0, ctypes.byref(p), stream))
+        self.ptr = p
+
+    def launch(self, stream=None):
+        _check(lib().khz_batch_launch(self.ptr, stream))
+
+    def wait(self, stream=None):
+        n = len(self.jobs)
+        counts = (ctypes.c_uint64 * (MAX_COUNTS * n))()
+        ext = (ctypes.c_uint64 * n)()
+        _check(lib().khz_batch_wait(self.ptr, counts, ext, stream))
+        return ([[int(counts[i * MAX_COUNTS + c]) for c in range(num_counts(app))]
+                 for i, (_, app) in enumerate(self.jobs)], [int(x) for x in ext])
+
+    def close(self):
+        if self.ptr:
+            lib().khz_batch_destroy(self.ptr)
+            self.ptr = None
 
 
 def count_noalloc(d_offsets, d_adj, n, num_entries, app, d_out, stream=None):

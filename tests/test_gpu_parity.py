@@ -219,15 +219,42 @@ def test_set_op_batch_matches_oracle(khz_ctx):
                 assert got[s:s + r].tolist() == buf[:r].tolist(), (op, i)
 
 
+BATCH_APPS = ["kautomine_triangle", "kautomine_four_clique", "kgraphpi_four_cycle", "kautomine_three_motif",
+              "kgraphpi_five_clique", "kautomine_four_motif"]
+
+
 def test_batch_matches_single(graphs, khz_ctx):
-    jobs = []
+    """Uneven batch (8 graphs x 6 apps, clique jobs on the bitmap engine, the rest on the DFS
+    engine, plus oriented inputs) in one launch sequence == one count per job."""
+    jobs, extra = [], []
     for spec, n, sym, off, adj, g in graphs:
-        for app in ["kautomine_triangle", "kautomine_four_clique", "kgraphpi_four_cycle", "kautomine_three_motif"]:
+        for app in BATCH_APPS:
             jobs.append((g, app))
+        og = khz_ctx.graph_from_edges(sym, n, orient=True)
+        extra.append(og)
+        jobs.append((og, "kautomine_four_clique"))
     counts, exts, st = khz_ctx.count_batch(jobs)
     for (g, app), c, e in zip(jobs, counts, exts):
         c1, st1 = khz_ctx.count(g, app)
         assert c == c1 and e == st1.num_extensions, app
+    for og in extra:
+        og.free()
+
+
+def test_batch_cuda_graph_replay(graphs, khz_ctx):
+    from openkhuzdulgraph_b200 import khz
+    jobs = [(g, app) for spec, n, sym, off, adj, g in graphs[:5] for app in BATCH_APPS]
+    expect = [khz_ctx.count(g, app) for g, app in jobs]
+    for cuda_graph in (False, True):
+        b = khz.Batch(khz_ctx, jobs, cuda_graph=cuda_graph)
+        try:
+            for _ in range(2):  # replays reuse the batch's scratch
+                b.launch()
+                counts, exts = b.wait()
+                for (c, st), c2, e2 in zip(expect, counts, exts):
+                    assert c == c2 and st.num_extensions == e2
+        finally:
+            b.close()
 
 
 def test_deterministic_repeat(graphs, khz_ctx):
