@@ -291,6 +291,82 @@ def ours(args, rank, world, local):
     ctx.close()
 
 
+BATCH_APPS = ["kautomine_triangle", "kautomine_four_clique", "kgraphpi_four_cycle", "kautomine_three_motif"]
+
+
+def batch_specs(n_graphs, seed=7):
+    """The uneven batch: vertex counts log-uniform in [64, 200000], average degree uniform in
+    [4, 40], one app each from BATCH_APPS.  A graph is R-MAT with scale = round(log2 n) and
+    edge factor = round(degree / 2) (2 * edge factor is the pre-dedupe average degree)."""
+    import math
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_graphs):
+        n = math.exp(rng.uniform(math.log(64), math.log(200000)))
+        deg = rng.uniform(4, 40)
+        scale = max(6, int(round(math.log2(n))))
+        ef = max(1, int(round(deg / 2)))
+        specs.append((scale, ef, 1000003 * seed + i, BATCH_APPS[int(rng.integers(0, len(BATCH_APPS)))]))
+    return specs
+
+
+def batch_workload(args):
+    """Plain (one khz_count per query, prepared launches cached) vs batched (all queries in one
+    launch sequence captured in a CUDA graph) on the same uneven batch."""
+    import torch
+    from openkhuzdulgraph_b200 import khz
+    torch.cuda.set_device(0)
+    ctx = khz.Context(0)
+    a, b, c = RMAT_ABC
+    t0 = time.time()
+    jobs, edges = [], 0
+    for scale, ef, seed, app in batch_specs(args.graphs):
+        g = ctx.generate_rmat(scale, ef, a, b, c, seed, orient=app in ("kautomine_triangle", "kautomine_four_clique"))
+        edges += g.num_entries
+        jobs.append((g, app))
+    t_gen = time.time() - t0
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    # plain: one query at a time (first pass prepares and caches each launch)
+    ref, emb = [], 0
+    for g, app in jobs:
+        cnt, st = ctx.count(g, app, stream=sptr)
+        ref.append(cnt)
+        emb += st.num_extensions + sum(cnt)
+    plain_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for (g, app), r in zip(jobs, ref):
+            cnt, _ = ctx.count(g, app, stream=sptr)
+            assert cnt == r
+        torch.cuda.synchronize()
+        plain_ms.append((time.perf_counter() - t1) * 1000)
+    batch = khz.Batch(ctx, jobs, cuda_graph=True, stream=sptr)
+    batch.launch(sptr)
+    counts, exts = batch.wait(sptr)
+    assert counts == ref
+    batch_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        batch.launch(sptr)
+        counts, _ = batch.wait(sptr)
+        batch_ms.append((time.perf_counter() - t1) * 1000)
+        assert counts == ref
+    batch.close()
+    p_ms, b_ms = statistics.median(plain_ms), statistics.median(batch_ms)
+    print(json.dumps({
+        "metric": "embeddings/s (uneven batch of %d graphs)" % len(jobs), "unit": "embeddings/s",
+        "value": emb / (b_ms / 1000), "plain_value": emb / (p_ms / 1000), "batched_over_plain": p_ms / b_ms,
+        "ms_batched": b_ms, "ms_plain": p_ms, "embeddings": emb, "graphs": len(jobs), "csr_entries": edges,
+        "generation_s": t_gen, "steps": args.steps, "higher_is_better": True, "data": "synthetic (device R-MAT)",
+        "config": {"workload": "uneven batch: n log-uniform [64, 200000], degree U[4, 40], "
+                               "apps %s" % BATCH_APPS}}), flush=True)
+    ctx.close()
+
+
 def reference_arm(args, rank, world, local):
     if rank != 0:
         return
@@ -325,9 +401,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident steps only (profiling)")
+    ap.add_argument("--workload", default="clique4", choices=["clique4", "batch"],
+                    help="clique4: the bench line; batch: the uneven multi-graph batch")
+    ap.add_argument("--graphs", type=int, default=20000, help="graphs in the batch workload")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the bench workload is 22)")
     ap.add_argument("--edge-factor", type=int, default=EDGE_FACTOR, help="R-MAT edge factor (workload: 16)")
     args = ap.parse_args()
+    if args.workload == "batch":
+        batch_workload(args)
+        return
     if args.impl == "reference":
         # the reference arm is a CPU run on rank 0; other ranks exit without work
         rank = int(os.environ.get("RANK", "0"))

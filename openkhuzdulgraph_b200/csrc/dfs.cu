@@ -121,6 +121,19 @@ __device__ uint32_t materialise(WarpCtx &c, const SetExpr &e, int dst, const Fil
     return r.full;
 }
 
+// Count-only `A op N(x)` filtered by f.  A subtraction is counted as |A passing f| minus
+// |A n N(x) passing f|, which probes the shorter of the two lists instead of all of A (the
+// instrumented variant keeps the reference's full subtraction so its byte count is the schedule's).
+template <bool STATS>
+__device__ __forceinline__ uint32_t count_op(WarpCtx &c, int8_t op, const uint32_t *A, uint32_t na, uint32_t x,
+                                            const Filter &f) {
+    if (!STATS && op == OP_SUB) {
+        const uint32_t pass_a = warp_count_plain(A, na, f);
+        return pass_a - apply_op<STATS>(c, OP_AND, A, na, x, nullptr, f, true).filtered;
+    }
+    return apply_op<STATS>(c, op, A, na, x, nullptr, f, true).filtered;
+}
+
 template <bool STATS>
 __device__ void count_last(WarpCtx &c) {
     const Plan &p = *c.plan;
@@ -135,7 +148,7 @@ __device__ void count_last(WarpCtx &c) {
         if (t.set.op[0] == OP_NONE) {
             cnt = warp_count_plain(A, na, f);
         } else if (t.set.op[1] == OP_NONE) {
-            cnt = apply_op<STATS>(c, t.set.op[0], A, na, c.v[t.set.op_arg[0]], nullptr, f, true).filtered;
+            cnt = count_op<STATS>(c, t.set.op[0], A, na, c.v[t.set.op_arg[0]], f);
         } else {
             const Filter none = {0, 0, 0, {0, 0, 0, 0}};
             // first op materialised (bounded by the term's lower bound when not instrumented)
@@ -143,8 +156,7 @@ __device__ void count_last(WarpCtx &c) {
             ProbeResult r0 = apply_op<STATS>(c, t.set.op[0], A, na, c.v[t.set.op_arg[0]], c.slot(5),
                                              STATS ? none : f, !STATS);
             __syncwarp();
-            cnt = apply_op<STATS>(c, t.set.op[1], c.slot(5), r0.full, c.v[t.set.op_arg[1]], nullptr, f, true)
-                      .filtered;
+            cnt = count_op<STATS>(c, t.set.op[1], c.slot(5), r0.full, c.v[t.set.op_arg[1]], f);
         }
         if (lane_id() == 0) c.acc[t.counter] += cnt;
     }
@@ -305,15 +317,20 @@ uint32_t round_cap(uint32_t slot_cap) { return slot_cap == 0 ? 32u : ((slot_cap 
 
 uint64_t dfs_total_warps(int warps_per_sm) { return (uint64_t)dfs_blocks(warps_per_sm) * kDfsWarpsPerBlock; }
 
-size_t dfs_arena_bytes(int n_jobs, int n_plans, uint64_t total_warps, uint32_t slot_cap) {
+uint64_t dfs_slot_words(int warps_per_sm, uint32_t slot_cap) {
+    return dfs_total_warps(warps_per_sm) * kNumSlots * round_cap(slot_cap);
+}
+
+size_t dfs_arena_bytes(int n_jobs, int n_plans, uint64_t total_warps, uint32_t slot_cap, bool own_slots) {
     return Arena::round(sizeof(DfsJob) * (size_t)std::max(n_jobs, 1)) +
            Arena::round(sizeof(Plan) * (size_t)std::max(n_plans, 4)) +
-           Arena::round(total_warps * kNumSlots * round_cap(slot_cap) * sizeof(uint32_t)) +
+           (own_slots ? Arena::round(total_warps * kNumSlots * round_cap(slot_cap) * sizeof(uint32_t)) : 0) +
            Arena::round(sizeof(unsigned long long));
 }
 
 khz_status dfs_prepare(const std::vector<DfsJob> &jobs, const std::vector<Plan> &plans, uint32_t slot_cap,
-                       int warps_per_sm, int chunk, bool stats, Arena *arena, DfsLaunch *dl, cudaStream_t s) {
+                       int warps_per_sm, int chunk, bool stats, bool own_slots, Arena *arena, DfsLaunch *dl,
+                       cudaStream_t s) {
     DfsLaunch L;
     L.n_jobs = (int)jobs.size();
     L.stats = stats;
@@ -325,9 +342,10 @@ khz_status dfs_prepare(const std::vector<DfsJob> &jobs, const std::vector<Plan> 
     DfsJob *d_jobs = arena->take<DfsJob>(jobs.size());
     // the kernel stages the first four plans into shared memory: keep at least four readable
     Plan *d_plans = arena->take<Plan>(std::max<size_t>(plans.size(), 4));
-    L.slots = arena->take<uint32_t>((size_t)L.blocks * kDfsWarpsPerBlock * kNumSlots * L.slot_cap);
+    L.slots = own_slots ? arena->take<uint32_t>((size_t)L.blocks * kDfsWarpsPerBlock * kNumSlots * L.slot_cap)
+                        : nullptr;
     L.queue = arena->take<unsigned long long>(1);
-    if (!d_jobs || !d_plans || !L.slots || !L.queue) {
+    if (!d_jobs || !d_plans || (own_slots && !L.slots) || !L.queue) {
         set_error("DFS launch arena too small");
         return KHZ_ERR_OOM;
     }
@@ -342,17 +360,22 @@ khz_status dfs_prepare(const std::vector<DfsJob> &jobs, const std::vector<Plan> 
     return KHZ_OK;
 }
 
-khz_status dfs_enqueue(const DfsLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls) {
+khz_status dfs_enqueue(const DfsLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls, uint32_t *slots) {
     if (L.n_jobs == 0 || L.total_units == 0) return KHZ_OK;
+    if (!slots) slots = L.slots;
+    if (!slots) {
+        set_error("DFS launch has no slot scratch");
+        return KHZ_ERR_ARG;
+    }
     KHZ_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(unsigned long long), s));
     uint64_t *pb = ls && ls->d_phase_bytes ? ls->d_phase_bytes + 3 : nullptr;
     if (ls && ls->ev_begin) cudaEventRecord(ls->ev_begin[3], s);
     if (L.stats)
-        dfs_kernel<true><<<L.blocks, L.threads, 0, s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk, L.slots,
+        dfs_kernel<true><<<L.blocks, L.threads, 0, s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk, slots,
                                                         L.slot_cap, L.queue, d_rows, pb);
     else
         dfs_kernel<false><<<L.blocks, L.threads, 0, s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk,
-                                                         L.slots, L.slot_cap, L.queue, d_rows, pb);
+                                                         slots, L.slot_cap, L.queue, d_rows, pb);
     KHZ_CUDA(cudaGetLastError());
     if (ls && ls->ev_begin) {
         cudaEventRecord(ls->ev_end[3], s);

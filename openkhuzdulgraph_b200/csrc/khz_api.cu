@@ -119,14 +119,16 @@ struct BatchPlan {
     uint64_t *d_raw = nullptr, *d_final = nullptr, *d_extadd = nullptr, *d_phase_bytes = nullptr;
     uint32_t *d_mult = nullptr;
     unsigned int *d_bad = nullptr;
-    uint64_t *h_final = nullptr;  // pinned: rows * kRowWords, then the bad flag
+    uint64_t *h_final = nullptr;  // pinned: rows * kRowWords, then the bad flag (own_scratch plans)
+    bool own_scratch = true;      // false: DFS slots and the pinned result buffer are the context's
+    uint64_t slot_words = 0;      // DFS slot words needed when they are shared
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~BatchPlan() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (mem) cudaFree(mem);
-        if (h_final) cudaFreeHost(h_final);
+        if (h_final && own_scratch) cudaFreeHost(h_final);
     }
 };
 
@@ -139,6 +141,10 @@ struct khz_ctx {
     cudaEvent_t ph_begin[kPhases] = {}, ph_end[kPhases] = {};
     cudaMemPool_t pool = nullptr;  // graphs and temporaries (keeps up to 4 GiB cached between calls)
     std::unordered_map<std::string, std::unique_ptr<BatchPlan>> plans;  // khz_count's prepared launches
+    // scratch shared by khz_count's launches, which the context serialises
+    uint32_t *shared_slots = nullptr;
+    uint64_t shared_slot_words = 0;
+    uint64_t *h_pinned = nullptr;  // kRowWords + 1 words
     std::mutex mu;
 };
 
@@ -204,7 +210,8 @@ int pick_engine(const khz_config &cfg, const AppDef &def, const Graph &g) {
     return engine;
 }
 
-khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, std::unique_ptr<BatchPlan> *out) {
+khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, bool own_scratch,
+                      std::unique_ptr<BatchPlan> *out) {
     if (n <= 0) {
         set_error("empty batch");
         return KHZ_ERR_ARG;
@@ -218,6 +225,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     }
     auto P = std::make_unique<BatchPlan>();
     P->rows = n;
+    P->own_scratch = own_scratch;
     P->stats = ctx->cfg.want_algo_bytes != 0;
     std::vector<BJob> bjobs;
     std::vector<DfsJob> djobs;
@@ -273,7 +281,8 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
                    Arena::round(sizeof(uint64_t) * n) + Arena::round(sizeof(unsigned int)) +
                    Arena::round(sizeof(uint64_t) * kPhases);
     if (P->has_bitmap) bytes += bitmap_arena_bytes((int)bjobs.size(), list_cap);
-    if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap);
+    if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
+    P->slot_words = P->has_dfs ? dfs_slot_words(ctx->cfg.dfs_warps_per_sm, slot_cap) : 0;
     cudaError_t e = cudaMalloc(&P->mem, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -296,10 +305,10 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, &P->arena, &P->bl, s);
     if (st) return st;
     if (P->has_dfs)
-        st = dfs_prepare(djobs, plans, slot_cap, ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, P->stats, &P->arena,
-                         &P->dl, s);
+        st = dfs_prepare(djobs, plans, slot_cap, ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, P->stats, own_scratch,
+                         &P->arena, &P->dl, s);
     if (st) return st;
-    if (cudaMallocHost(&P->h_final, sizeof(uint64_t) * ((size_t)kRowWords * n + 1)) != cudaSuccess) {
+    if (own_scratch && cudaMallocHost(&P->h_final, sizeof(uint64_t) * ((size_t)kRowWords * n + 1)) != cudaSuccess) {
         cudaGetLastError();
         P->h_final = nullptr;
         set_error("pinned result buffer allocation failed");
@@ -312,7 +321,8 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
 
 // Enqueue the plan: zero the counters, the engines' launches, finalize.  `ls` (may be null)
 // records per-phase events; ev_begin / ev_end (may be null) bracket the counting launches.
-khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent_t ev_begin, cudaEvent_t ev_end) {
+khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent_t ev_begin, cudaEvent_t ev_end,
+                        uint32_t *shared_slots = nullptr) {
     KHZ_CUDA(cudaMemsetAsync(P->d_raw, 0, sizeof(uint64_t) * kRowWords * P->rows, s));
     KHZ_CUDA(cudaMemsetAsync(P->d_bad, 0, sizeof(unsigned int), s));
     KHZ_CUDA(cudaMemsetAsync(P->d_phase_bytes, 0, sizeof(uint64_t) * kPhases, s));
@@ -321,7 +331,7 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
     khz_status st = KHZ_OK;
     if (P->has_bitmap) st = bitmap_enqueue(P->bl, P->d_raw, s, ls);
     if (st) return st;
-    if (P->has_dfs) st = dfs_enqueue(P->dl, P->d_raw, s, ls);
+    if (P->has_dfs) st = dfs_enqueue(P->dl, P->d_raw, s, ls, P->own_scratch ? nullptr : shared_slots);
     if (st) return st;
     if (ev_end) KHZ_CUDA(cudaEventRecord(ev_end, s));
     finalize_kernel<<<(unsigned)((P->rows + 127) / 128), 128, 0, s>>>(P->d_raw, P->rows, P->d_mult, P->d_extadd,
@@ -331,8 +341,10 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
     return KHZ_OK;
 }
 
-// copy the finalized rows to the plan's pinned buffer and wait for them
-khz_status read_plan(BatchPlan *P, cudaStream_t s) {
+// copy the finalized rows to pinned memory (the plan's, or `host` for shared-scratch plans)
+// and wait for them
+khz_status read_plan(BatchPlan *P, cudaStream_t s, uint64_t *host = nullptr) {
+    if (host) P->h_final = host;
     const size_t words = (size_t)kRowWords * P->rows;
     KHZ_CUDA(cudaMemcpyAsync(P->h_final, P->d_final, sizeof(uint64_t) * words, cudaMemcpyDeviceToHost, s));
     KHZ_CUDA(cudaMemcpyAsync(P->h_final + words, P->d_bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
@@ -387,10 +399,36 @@ khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, Batch
     }
     khz_job j{g, (int32_t)app, 0};
     std::unique_ptr<BatchPlan> P;
-    khz_status st = build_plan(ctx, &j, 1, s, &P);
+    khz_status st = build_plan(ctx, &j, 1, s, false, &P);
     if (st) return st;
     *out = P.get();
     ctx->plans[key] = std::move(P);
+    return KHZ_OK;
+}
+
+// the context's shared DFS slots (>= words) and pinned result buffer
+khz_status ensure_shared(khz_ctx *ctx, uint64_t words) {
+    if (!ctx->h_pinned) {
+        if (cudaMallocHost(&ctx->h_pinned, sizeof(uint64_t) * (kRowWords + 1)) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->h_pinned = nullptr;
+            set_error("pinned result buffer allocation failed");
+            return KHZ_ERR_OOM;
+        }
+    }
+    if (words > ctx->shared_slot_words) {
+        if (ctx->shared_slots) cudaFree(ctx->shared_slots);  // waits for work still using it
+        ctx->shared_slots = nullptr;
+        ctx->shared_slot_words = 0;
+        cudaError_t e = cudaMalloc(&ctx->shared_slots, sizeof(uint32_t) * words);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ctx->shared_slots = nullptr;
+            set_error("DFS scratch of %llu bytes: %s", (unsigned long long)(4 * words), cudaGetErrorString(e));
+            return KHZ_ERR_OOM;
+        }
+        ctx->shared_slot_words = words;
+    }
     return KHZ_OK;
 }
 
@@ -459,6 +497,8 @@ khz_status khz_ctx_destroy(khz_ctx *ctx) {
     }
     cudaDeviceSynchronize();
     ctx->plans.clear();
+    if (ctx->shared_slots) cudaFree(ctx->shared_slots);
+    if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -751,7 +791,9 @@ khz_status khz_count_async(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *
     BatchPlan *P = nullptr;
     st = cached_plan(ctx, g, app, s, &P);
     if (st) return st;
-    st = enqueue_plan(P, s, nullptr, nullptr, nullptr);
+    st = ensure_shared(ctx, P->slot_words);
+    if (st) return st;
+    st = enqueue_plan(P, s, nullptr, nullptr, nullptr, ctx->shared_slots);
     if (st) return st;
     KHZ_CUDA(cudaMemcpyAsync(d_out, P->d_final, sizeof(uint64_t) * kRowWords, cudaMemcpyDeviceToDevice, s));
     return KHZ_OK;
@@ -769,12 +811,14 @@ khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts
     BatchPlan *P = nullptr;
     st = cached_plan(ctx, g, app, s, &P);
     if (st) return st;
+    st = ensure_shared(ctx, P->slot_words);
+    if (st) return st;
     LaunchStats ls;
     ls.ev_begin = ctx->ph_begin;
     ls.ev_end = ctx->ph_end;
-    st = enqueue_plan(P, s, &ls, ctx->ev0, ctx->ev1);
+    st = enqueue_plan(P, s, &ls, ctx->ev0, ctx->ev1, ctx->shared_slots);
     if (st) return st;
-    st = read_plan(P, s);
+    st = read_plan(P, s, ctx->h_pinned);
     if (st) return st;
     const int nc = app_def(app).num_counts;
     for (int c = 0; c < nc; ++c) counts[c] = P->h_final[c];
@@ -793,7 +837,7 @@ khz_status khz_count_batch(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
     std::unique_ptr<BatchPlan> P;
-    st = build_plan(ctx, jobs, n_jobs, s, &P);
+    st = build_plan(ctx, jobs, n_jobs, s, true, &P);
     if (st) return st;
     LaunchStats ls;
     ls.ev_begin = ctx->ph_begin;
@@ -822,7 +866,7 @@ khz_status khz_batch_create(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint3
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
     std::unique_ptr<khz_batch> b(new khz_batch{ctx, nullptr});
-    st = build_plan(ctx, jobs, n_jobs, s, &b->plan);
+    st = build_plan(ctx, jobs, n_jobs, s, true, &b->plan);
     if (st) return st;
     if (flags & KHZ_BATCH_CUDA_GRAPH) {
         cudaStream_t cs = nullptr;

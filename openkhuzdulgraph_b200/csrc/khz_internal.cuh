@@ -199,10 +199,15 @@ struct LaunchStats {
 // DFS engine.  Jobs carry unit_begin (prefix of num_units); rows of kRowWords uint64 must be
 // zeroed by the caller.  No host synchronisation in dfs_enqueue.
 uint64_t dfs_total_warps(int warps_per_sm);
-size_t dfs_arena_bytes(int n_jobs, int n_plans, uint64_t total_warps, uint32_t slot_cap);
+// slot scratch is either owned by the launch (own_slots) or passed to dfs_enqueue by the caller
+// (dfs_slot_words words), e.g. one buffer shared by launches that never overlap
+uint64_t dfs_slot_words(int warps_per_sm, uint32_t slot_cap);
+size_t dfs_arena_bytes(int n_jobs, int n_plans, uint64_t total_warps, uint32_t slot_cap, bool own_slots);
 khz_status dfs_prepare(const std::vector<DfsJob> &jobs, const std::vector<Plan> &plans, uint32_t slot_cap,
-                       int warps_per_sm, int chunk, bool stats, Arena *arena, DfsLaunch *dl, cudaStream_t s);
-khz_status dfs_enqueue(const DfsLaunch &dl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
+                       int warps_per_sm, int chunk, bool stats, bool own_slots, Arena *arena, DfsLaunch *dl,
+                       cudaStream_t s);
+khz_status dfs_enqueue(const DfsLaunch &dl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls,
+                       uint32_t *slots = nullptr);
 khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_plans, uint64_t total_units,
                                uint32_t chunk, uint32_t *slots, uint32_t slot_cap, unsigned long long *queue,
                                uint64_t *d_raw, int blocks, int threads, cudaStream_t s);
