@@ -518,7 +518,9 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     for (int t = 0; t < 2; ++t) {
         const size_t smem = block_smem(dcaps[t]);
         auto kern = stats ? clique_block_kernel<true> : clique_block_kernel<false>;
-        KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // the attribute is per kernel, shared by every prepared launch: always allow the largest
+        // footprint so launches prepared earlier with more shared memory stay valid
+        KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem(kBlockMax)));
         int per_sm = 0;
         KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
         L.block_smem[t] = smem;

@@ -316,6 +316,13 @@ def test_bitmap_large_tier_matches_oracle(khz_ctx):
             exp, ext, _ = orc.count(app, ooff, oadj)
             assert got == exp and st.num_extensions == ext, app
             assert st.phase_launches[2] == 1  # the large tier ran
+        # a launch prepared later with less shared memory must not invalidate this graph's cached one
+        canon2, n2 = orc.rmat(9, 16, seed=3)
+        small = khz_ctx.graph_from_edges(orc.symmetrize(canon2), n2, orient=True)
+        khz_ctx.count(small, "kautomine_four_clique")
+        small.free()
+        got, st = khz_ctx.count(og, "kautomine_four_clique")
+        assert got == orc.count("kautomine_four_clique", ooff, oadj)[0]
         khz_ctx.set_config(engine=khz.ENGINE_BITMAP)
         b5, sb = khz_ctx.count(og, "kautomine_five_clique")
         khz_ctx.set_config(engine=khz.ENGINE_DFS)
