@@ -367,6 +367,118 @@ def batch_workload(args):
     ctx.close()
 
 
+SERVE_APPS = ["kautomine_triangle", "kautomine_four_clique", "kautomine_five_clique", "kgraphpi_four_cycle",
+              "kgraphpi_house", "kautomine_four_motif"]
+
+
+def serve_graph_specs(n_graphs=64, e_min=1e3, e_max=5e8):
+    """R-MAT (scale, edge factor) whose raw edge count ef * 2^scale is log-spaced over [e_min, e_max]
+    (the largest is scale 24, edge factor 32)."""
+    import math
+    specs = []
+    for i in range(n_graphs):
+        e = e_min * (e_max / e_min) ** (i / (n_graphs - 1))
+        scale = min(24, max(6, int(round(math.log2(e / 16)))))
+        ef = max(1, int(round(e / 2 ** scale)))
+        specs.append((scale, ef, 5000 + i))
+    return specs
+
+
+def serve_workload(args):
+    """Poisson arrivals of counting queries against 64 device-resident graphs; p50/p99 latency and
+    throughput of the continuous-batching server, and its saturated throughput against plain
+    one-query-at-a-time counting on the same query list."""
+    import random
+    import threading
+    import torch
+    from openkhuzdulgraph_b200 import khz
+    torch.cuda.set_device(0)
+    ctx = khz.Context(0)
+    a, b, c = RMAT_ABC
+    t0 = time.time()
+    graphs = [ctx.generate_rmat(sc, ef, a, b, c, seed) for sc, ef, seed in serve_graph_specs()]
+    sizes = [g.num_entries // 2 for g in graphs]
+    t_gen = time.time() - t0
+    # feasibility: per app, graphs in increasing size until one query alone exceeds the cap
+    feasible, alone = [], {}
+    for app in SERVE_APPS:
+        for gi, g in enumerate(graphs):
+            t1 = time.perf_counter()
+            cnt, st = ctx.count(g, app)
+            dt = (time.perf_counter() - t1) * 1000
+            alone[(gi, app)] = (cnt, st.num_extensions, dt)
+            if dt > args.query_cap_ms:
+                break
+            feasible.append((gi, app))
+    rng = random.Random(11)
+    sv = khz.Server(ctx, slots=args.slots, max_batch=args.max_batch)
+    # warm: every feasible query once through the server
+    for gi, app in feasible:
+        sv.wait(sv.submit(graphs[gi], app), app)
+    rates_out = []
+    for rate in args.rates:
+        sv.reset_stats()
+        n_q = max(50, int(rate * args.duration))
+        qs = [rng.choice(feasible) for _ in range(n_q)]
+        arrivals = []
+        t = 0.0
+        for _ in qs:
+            t += rng.expovariate(rate)
+            arrivals.append(t)
+        tickets = [None] * n_q
+
+        def submitter():
+            start = time.perf_counter()
+            for k, ((gi, app), ta) in enumerate(zip(qs, arrivals)):
+                d = ta - (time.perf_counter() - start)
+                if d > 0:
+                    time.sleep(d)
+                tickets[k] = sv.submit(graphs[gi], app)
+
+        th = threading.Thread(target=submitter)
+        ts = time.perf_counter()
+        th.start()
+        lat = []
+        for k in range(n_q):
+            while tickets[k] is None:
+                time.sleep(0.0002)
+            gi, app = qs[k]
+            cnt, ext, l = sv.wait(tickets[k], app, timeout_ms=600000.0)
+            assert cnt == alone[(gi, app)][0] and ext == alone[(gi, app)][1]
+            lat.append(l)
+        th.join()
+        wall = time.perf_counter() - ts
+        lat.sort()
+        rates_out.append({"offered_qps": rate, "queries": n_q, "achieved_qps": n_q / wall,
+                          "p50_ms": lat[len(lat) // 2], "p99_ms": lat[int(0.99 * (len(lat) - 1))],
+                          "batches": sv.stats()["batches"]})
+    # saturation: the same 2000-query list submitted at once vs plain sequential counting
+    qs = [rng.choice(feasible) for _ in range(args.sat_queries)]
+    sv.reset_stats()
+    t1 = time.perf_counter()
+    tk = [sv.submit(graphs[gi], app) for gi, app in qs]
+    for (gi, app), t in zip(qs, tk):
+        sv.wait(t, app, timeout_ms=600000.0)
+    served_s = time.perf_counter() - t1
+    sv.close()
+    t1 = time.perf_counter()
+    for gi, app in qs:
+        ctx.count(graphs[gi], app)
+    plain_s = time.perf_counter() - t1
+    out = {"metric": "served queries/s and latency (continuous batching)", "unit": "queries/s",
+           "value": len(qs) / served_s, "plain_value": len(qs) / plain_s, "served_over_plain": plain_s / served_s,
+           "rates": rates_out, "graphs": len(graphs), "undirected_edges_total": int(sum(sizes)),
+           "largest_graph_edges": int(max(sizes)), "feasible_queries": len(feasible),
+           "feasible_per_app": {app: sum(1 for _, a2 in feasible if a2 == app) for app in SERVE_APPS},
+           "query_cap_ms": args.query_cap_ms, "slots": args.slots, "max_batch": args.max_batch,
+           "generation_s": t_gen, "data": "synthetic (device R-MAT)", "higher_is_better": True,
+           "config": {"workload": "serving: Poisson arrivals, 64 resident R-MAT graphs with 1e3..5e8 raw edges "
+                                  "(log-spaced), apps %s; a (graph, app) pair is served when that query alone "
+                                  "takes <= query_cap_ms" % SERVE_APPS}}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def reference_arm(args, rank, world, local):
     if rank != 0:
         return
@@ -401,14 +513,23 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident steps only (profiling)")
-    ap.add_argument("--workload", default="clique4", choices=["clique4", "batch"],
-                    help="clique4: the bench line; batch: the uneven multi-graph batch")
+    ap.add_argument("--workload", default="clique4", choices=["clique4", "batch", "serve"],
+                    help="clique4: the bench line; batch: the uneven multi-graph batch; serve: Poisson serving")
+    ap.add_argument("--rates", type=float, nargs="+", default=[100, 500, 1000, 2000, 5000])
+    ap.add_argument("--duration", type=float, default=2.0, help="seconds of arrivals per rate (serve)")
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--max-batch", type=int, default=64)
+    ap.add_argument("--query-cap-ms", type=float, default=100.0)
+    ap.add_argument("--sat-queries", type=int, default=2000)
     ap.add_argument("--graphs", type=int, default=20000, help="graphs in the batch workload")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the bench workload is 22)")
     ap.add_argument("--edge-factor", type=int, default=EDGE_FACTOR, help="R-MAT edge factor (workload: 16)")
     args = ap.parse_args()
     if args.workload == "batch":
         batch_workload(args)
+        return
+    if args.workload == "serve":
+        serve_workload(args)
         return
     if args.impl == "reference":
         # the reference arm is a CPU run on rank 0; other ranks exit without work

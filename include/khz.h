@@ -178,6 +178,34 @@ khz_status khz_batch_launch(khz_batch *batch, void *stream);
 khz_status khz_batch_wait(khz_batch *batch, uint64_t *counts, uint64_t *num_ext, void *stream);
 khz_status khz_batch_destroy(khz_batch *batch);
 
+/* ---- serving: continuous batching of counting queries ----------------------------- */
+/* A server owns `slots` CUDA streams and a scheduler thread.  Queries (graph, app) are admitted in
+ * arrival order as slots and HBM budget free up (a query's footprint is its engine scratch: DFS
+ * stacks sized by the graph's largest degree, or the bitmap engine's start-vertex lists; graphs
+ * are resident and not counted); up to `max_batch` admitted queries share one launch sequence;
+ * different slots' work overlaps on the device.  hbm_budget 0 = half the free device memory.
+ * Replaces nothing in the reference (its engine serves one run() at a time). */
+typedef struct khz_server khz_server;
+typedef uint64_t khz_ticket;
+typedef struct khz_server_stats {
+    uint64_t completed;          /* queries finished since creation / the last reset */
+    uint64_t batches;            /* launch sequences dispatched */
+    uint64_t pending;            /* queries waiting for admission */
+    uint64_t max_bytes_in_flight;/* largest admitted scratch footprint seen */
+    double p50_ms, p99_ms, max_ms;  /* submit-to-result latency */
+    double queries_per_s;        /* completed / (last completion - first submission) */
+} khz_server_stats;
+khz_status khz_server_create(khz_ctx *ctx, int slots, int max_batch, uint64_t hbm_budget, khz_server **out);
+khz_status khz_server_submit(khz_server *server, khz_graph g, khz_app_id app, khz_ticket *ticket);
+/* Waits up to timeout_ms (0: poll) for the ticket; KHZ_ERR_BUSY (poll) / KHZ_ERR_TIMEOUT if not done.
+ * A finished ticket is consumed by the call that returns its result. */
+khz_status khz_server_wait(khz_server *server, khz_ticket ticket, uint64_t *counts, uint64_t *num_ext,
+                           double *latency_ms, double timeout_ms);
+khz_status khz_server_stats_get(khz_server *server, khz_server_stats *stats);
+khz_status khz_server_reset_stats(khz_server *server);
+/* Finishes every submitted query, then releases the server. */
+khz_status khz_server_destroy(khz_server *server);
+
 /* ---- VertexSet algebra as a batch (test / tool entry) ----------------------------- */
 /* VertexSet::intersect_with / subtracted_by / intersect_and_count / bounded_* and the
  * trims (vertex_set.cc:20-184, utilities.h:64-86) over n_pairs independent pairs of

@@ -5,7 +5,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <memory>
+#include <thread>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -120,15 +124,21 @@ struct BatchPlan {
     uint32_t *d_mult = nullptr;
     unsigned int *d_bad = nullptr;
     uint64_t *h_final = nullptr;  // pinned: rows * kRowWords, then the bad flag (own_scratch plans)
-    bool own_scratch = true;      // false: DFS slots and the pinned result buffer are the context's
+    bool own_scratch = true;      // false: DFS slots are the context's shared ones
+    bool own_pinned = false;      // h_final was allocated by the plan
     uint64_t slot_words = 0;      // DFS slot words needed when they are shared
+    size_t mem_bytes = 0;
+    cudaStream_t pool_stream = nullptr;  // mem came from the context pool, freed on this stream
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~BatchPlan() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        if (mem) cudaFree(mem);
-        if (h_final && own_scratch) cudaFreeHost(h_final);
+        if (mem) {
+            if (pool_stream) cudaFreeAsync(mem, pool_stream);
+            else cudaFree(mem);
+        }
+        if (h_final && own_pinned) cudaFreeHost(h_final);
     }
 };
 
@@ -152,6 +162,60 @@ struct khz_batch {
     khz_ctx *ctx;
     std::unique_ptr<BatchPlan> plan;
 };
+
+// ------------------------------------------------------------------------------------------
+// Serving: continuous batching of counting queries on device-resident graphs.
+// A scheduler thread owns S slots (CUDA streams).  Whenever a slot is free it admits the oldest
+// pending queries whose estimated scratch footprint fits the remaining HBM budget, prepares one
+// launch sequence for them (scratch from the context's stream-ordered pool) and enqueues it on the
+// slot's stream; work of different slots overlaps on the device.  Completion is detected with
+// events; results and submit-to-result latencies are handed back through tickets.
+// ------------------------------------------------------------------------------------------
+struct ServeRequest {
+    khz_ticket id;
+    khz_graph graph;
+    int app;
+    double t_submit;  // seconds, steady clock
+    uint64_t footprint;
+};
+
+struct ServeResult {
+    bool done = false;
+    khz_status status = KHZ_OK;
+    uint64_t counts[KHZ_MAX_COUNTS] = {};
+    uint64_t num_ext = 0;
+    double latency_ms = 0;
+};
+
+struct ServeSlot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    std::unique_ptr<BatchPlan> plan;
+    std::vector<ServeRequest> reqs;
+    uint64_t *h_rows = nullptr;  // pinned: max_batch * kRowWords + 1
+    uint64_t footprint = 0;
+    bool busy = false;
+};
+
+struct khz_server {
+    khz_ctx *ctx = nullptr;
+    int max_batch = 64;
+    uint64_t budget = 0, in_use = 0;
+    std::vector<ServeSlot> slots;
+    std::deque<ServeRequest> pending;
+    std::unordered_map<khz_ticket, ServeResult> results;
+    std::unordered_map<uint64_t, uint64_t> footprints;  // (graph, app) -> bytes, guarded by fp_mu
+    std::mutex fp_mu;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread worker;
+    bool stop = false;
+    khz_ticket next_ticket = 1;
+    std::vector<double> latencies;
+    uint64_t completed = 0, batches = 0, max_in_flight = 0;
+    double t_first = -1, t_last = 0;
+};
+
 
 namespace {
 
@@ -210,8 +274,14 @@ int pick_engine(const khz_config &cfg, const AppDef &def, const Graph &g) {
     return engine;
 }
 
-khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, bool own_scratch,
+// build options
+constexpr unsigned kPlanOwnSlots = 1u;   // the plan owns its DFS slots (else the context's shared ones)
+constexpr unsigned kPlanPinned = 2u;     // the plan owns a pinned result buffer
+constexpr unsigned kPlanPoolMem = 4u;    // device scratch from the context's stream-ordered pool on `s`
+
+khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, unsigned opts,
                       std::unique_ptr<BatchPlan> *out) {
+    const bool own_scratch = (opts & kPlanOwnSlots) != 0;
     if (n <= 0) {
         set_error("empty batch");
         return KHZ_ERR_ARG;
@@ -283,7 +353,14 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     if (P->has_bitmap) bytes += bitmap_arena_bytes((int)bjobs.size(), list_cap);
     if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
     P->slot_words = P->has_dfs ? dfs_slot_words(ctx->cfg.dfs_warps_per_sm, slot_cap) : 0;
-    cudaError_t e = cudaMalloc(&P->mem, bytes);
+    cudaError_t e;
+    if (opts & kPlanPoolMem) {
+        e = cudaMallocFromPoolAsync(&P->mem, bytes, ctx->pool, s);
+        if (e == cudaSuccess) P->pool_stream = s;
+    } else {
+        e = cudaMalloc(&P->mem, bytes);
+    }
+    P->mem_bytes = bytes;
     if (e != cudaSuccess) {
         cudaGetLastError();
         P->mem = nullptr;
@@ -308,12 +385,14 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         st = dfs_prepare(djobs, plans, slot_cap, ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, P->stats, own_scratch,
                          &P->arena, &P->dl, s);
     if (st) return st;
-    if (own_scratch && cudaMallocHost(&P->h_final, sizeof(uint64_t) * ((size_t)kRowWords * n + 1)) != cudaSuccess) {
+    if ((opts & kPlanPinned) &&
+        cudaMallocHost(&P->h_final, sizeof(uint64_t) * ((size_t)kRowWords * n + 1)) != cudaSuccess) {
         cudaGetLastError();
         P->h_final = nullptr;
         set_error("pinned result buffer allocation failed");
         return KHZ_ERR_OOM;
     }
+    P->own_pinned = (opts & kPlanPinned) != 0;
     KHZ_CUDA(cudaStreamSynchronize(s));
     *out = std::move(P);
     return KHZ_OK;
@@ -399,7 +478,7 @@ khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, Batch
     }
     khz_job j{g, (int32_t)app, 0};
     std::unique_ptr<BatchPlan> P;
-    khz_status st = build_plan(ctx, &j, 1, s, false, &P);
+    khz_status st = build_plan(ctx, &j, 1, s, 0, &P);
     if (st) return st;
     *out = P.get();
     ctx->plans[key] = std::move(P);
@@ -430,6 +509,158 @@ khz_status ensure_shared(khz_ctx *ctx, uint64_t words) {
         ctx->shared_slot_words = words;
     }
     return KHZ_OK;
+}
+
+
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// HBM scratch one query needs while it runs: DFS slots sized by the graph's largest degree, or
+// the bitmap engine's start-vertex lists; the CSR itself is resident and not counted
+khz_status serve_footprint(khz_server *sv, khz_graph h, int app, uint64_t *bytes) {
+    const uint64_t key = ((uint64_t)h << 8) | (uint64_t)app;
+    std::lock_guard<std::mutex> fl(sv->fp_mu);  // lock order: fp_mu, then ctx->mu; never sv->mu here
+    auto it = sv->footprints.find(key);
+    if (it != sv->footprints.end()) {
+        *bytes = it->second;
+        return KHZ_OK;
+    }
+    khz_ctx *ctx = sv->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Graph *g = get_graph(ctx, h);
+    if (!g) return KHZ_ERR_ARG;
+    const AppDef &def = app_def(app);
+    uint64_t b = 1ull << 16;
+    if (pick_engine(ctx->cfg, def, *g) == KHZ_ENGINE_BITMAP) {
+        Graph *og = nullptr;
+        khz_status st = oriented_of(ctx, h, &og, nullptr);  // orient once, before any timing matters
+        if (st) return st;
+        b += 2 * 4 * (og->m / 65 + 1);
+        if (og->max_degree > bitmap_block_max_degree())
+            b += 4 * dfs_slot_words(ctx->cfg.dfs_warps_per_sm, og->max_degree);
+    } else {
+        b += 4 * dfs_slot_words(ctx->cfg.dfs_warps_per_sm, g->max_degree);
+    }
+    sv->footprints[key] = b;
+    *bytes = b;
+    return KHZ_OK;
+}
+
+// finish every slot whose work is done; returns true if any slot is still busy
+bool serve_reap(khz_server *sv) {
+    bool any_busy = false;
+    for (auto &sl : sv->slots) {
+        if (!sl.busy) continue;
+        const cudaError_t q = cudaEventQuery(sl.done);
+        if (q == cudaErrorNotReady) {
+            any_busy = true;
+            continue;
+        }
+        const double t = now_s();
+        khz_status st = KHZ_OK;
+        if (q != cudaSuccess) st = cuda_fail(q, "serving slot");
+        const size_t words = (size_t)kRowWords * sl.reqs.size();
+        if (st == KHZ_OK && *(const unsigned int *)(sl.h_rows + words)) st = KHZ_ERR_MULTIPLICITY;
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            for (size_t i = 0; i < sl.reqs.size(); ++i) {
+                ServeResult &r = sv->results[sl.reqs[i].id];
+                r.status = st;
+                for (int c = 0; c < KHZ_MAX_COUNTS; ++c) r.counts[c] = sl.h_rows[i * kRowWords + c];
+                r.num_ext = sl.h_rows[i * kRowWords + KHZ_MAX_COUNTS];
+                r.latency_ms = (t - sl.reqs[i].t_submit) * 1000.0;
+                r.done = true;
+                sv->latencies.push_back(r.latency_ms);
+                sv->completed += 1;
+            }
+            sv->t_last = t;
+            sv->in_use -= sl.footprint;
+        }
+        sl.plan.reset();  // returns the scratch to the pool, ordered on the slot's stream
+        sl.reqs.clear();
+        sl.busy = false;
+        sv->cv_done.notify_all();
+    }
+    return any_busy;
+}
+
+// admit pending queries into idle slots
+void serve_dispatch(khz_server *sv) {
+    for (auto &sl : sv->slots) {
+        if (sl.busy) continue;
+        std::vector<ServeRequest> take;
+        uint64_t fp = 0;
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            while (!sv->pending.empty() && (int)take.size() < sv->max_batch) {
+                const ServeRequest &r = sv->pending.front();
+                const bool fits = sv->in_use + fp + r.footprint <= sv->budget;
+                // a query larger than the whole budget still runs, alone, when nothing else does
+                if (!fits && !(take.empty() && sv->in_use == 0)) break;
+                fp += r.footprint;
+                take.push_back(r);
+                sv->pending.pop_front();
+            }
+            if (take.empty()) return;
+            sv->in_use += fp;
+            sv->max_in_flight = std::max<uint64_t>(sv->max_in_flight, sv->in_use);
+        }
+        std::vector<khz_job> jobs(take.size());
+        for (size_t i = 0; i < take.size(); ++i) jobs[i] = khz_job{take[i].graph, (int32_t)take[i].app, 0};
+        khz_status st;
+        {
+            std::lock_guard<std::mutex> lk(sv->ctx->mu);
+            st = build_plan(sv->ctx, jobs.data(), (int)jobs.size(), sl.stream, kPlanOwnSlots | kPlanPoolMem,
+                            &sl.plan);
+        }
+        if (st == KHZ_OK) st = enqueue_plan(sl.plan.get(), sl.stream, nullptr, nullptr, nullptr);
+        if (st == KHZ_OK) {
+            const size_t words = (size_t)kRowWords * take.size();
+            cudaError_t e = cudaMemcpyAsync(sl.h_rows, sl.plan->d_final, sizeof(uint64_t) * words,
+                                            cudaMemcpyDeviceToHost, sl.stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(sl.h_rows + words, sl.plan->d_bad, sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                    sl.stream);
+            if (e == cudaSuccess) e = cudaEventRecord(sl.done, sl.stream);
+            if (e != cudaSuccess) st = cuda_fail(e, "serving dispatch");
+        }
+        if (st != KHZ_OK) {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            for (auto &r : take) {
+                ServeResult &res = sv->results[r.id];
+                res.status = st;
+                res.done = true;
+            }
+            sv->in_use -= fp;
+            sl.plan.reset();
+            sv->cv_done.notify_all();
+            continue;
+        }
+        sl.reqs = std::move(take);
+        sl.footprint = fp;
+        sl.busy = true;
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->batches += 1;
+    }
+}
+
+void serve_loop(khz_server *sv) {
+    cudaSetDevice(sv->ctx->device);
+    while (true) {
+        serve_reap(sv);
+        serve_dispatch(sv);
+        bool busy = false;
+        for (const auto &sl : sv->slots) busy = busy || sl.busy;
+        std::unique_lock<std::mutex> lk(sv->mu);
+        if (sv->stop && sv->pending.empty() && !busy) break;
+        if (sv->pending.empty() && !busy) {
+            sv->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+        } else {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    }
 }
 
 }  // namespace
@@ -837,7 +1068,7 @@ khz_status khz_count_batch(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
     std::unique_ptr<BatchPlan> P;
-    st = build_plan(ctx, jobs, n_jobs, s, true, &P);
+    st = build_plan(ctx, jobs, n_jobs, s, kPlanOwnSlots | kPlanPinned, &P);
     if (st) return st;
     LaunchStats ls;
     ls.ev_begin = ctx->ph_begin;
@@ -866,7 +1097,7 @@ khz_status khz_batch_create(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint3
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
     std::unique_ptr<khz_batch> b(new khz_batch{ctx, nullptr});
-    st = build_plan(ctx, jobs, n_jobs, s, true, &b->plan);
+    st = build_plan(ctx, jobs, n_jobs, s, kPlanOwnSlots | kPlanPinned, &b->plan);
     if (st) return st;
     if (flags & KHZ_BATCH_CUDA_GRAPH) {
         cudaStream_t cs = nullptr;
@@ -923,6 +1154,159 @@ khz_status khz_batch_destroy(khz_batch *b) {
     cudaSetDevice(b->ctx->device);
     cudaDeviceSynchronize();
     delete b;
+    return KHZ_OK;
+}
+
+
+khz_status khz_server_create(khz_ctx *ctx, int slots, int max_batch, uint64_t hbm_budget, khz_server **out) {
+    khz_status st = check_ctx(ctx);
+    if (st) return st;
+    if (!out || slots < 1 || slots > 64 || max_batch < 1) {
+        set_error("server needs 1..64 slots and max_batch >= 1");
+        return KHZ_ERR_ARG;
+    }
+    std::unique_ptr<khz_server> sv(new khz_server());
+    sv->ctx = ctx;
+    sv->max_batch = max_batch;
+    if (hbm_budget == 0) {
+        size_t free_b = 0, total_b = 0;
+        KHZ_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        hbm_budget = free_b / 2;
+    }
+    sv->budget = hbm_budget;
+    sv->slots.resize(slots);
+    for (auto &sl : sv->slots) {
+        KHZ_CUDA(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+        KHZ_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+        if (cudaMallocHost(&sl.h_rows, sizeof(uint64_t) * ((size_t)kRowWords * max_batch + 1)) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("pinned result buffer allocation failed");
+            return KHZ_ERR_OOM;
+        }
+    }
+    khz_server *p = sv.get();
+    sv->worker = std::thread([p] { serve_loop(p); });
+    *out = sv.release();
+    return KHZ_OK;
+}
+
+khz_status khz_server_submit(khz_server *sv, khz_graph g, khz_app_id app, khz_ticket *ticket) {
+    if (!sv || !ticket) {
+        set_error("null argument");
+        return KHZ_ERR_ARG;
+    }
+    if (app < 0 || app >= KHZ_NUM_APPS) {
+        set_error("invalid app id %d", (int)app);
+        return KHZ_ERR_ARG;
+    }
+    cudaSetDevice(sv->ctx->device);
+    uint64_t fp = 0;
+    khz_status st;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        if (sv->stop) {
+            set_error("server is shutting down");
+            return KHZ_ERR_BUSY;
+        }
+    }
+    st = serve_footprint(sv, g, app, &fp);
+    if (st) return st;
+    const double t = now_s();
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        const khz_ticket id = sv->next_ticket++;
+        sv->pending.push_back(ServeRequest{id, g, (int)app, t, fp});
+        sv->results[id] = ServeResult{};
+        if (sv->t_first < 0) sv->t_first = t;
+        *ticket = id;
+    }
+    sv->cv_work.notify_one();
+    return KHZ_OK;
+}
+
+khz_status khz_server_wait(khz_server *sv, khz_ticket ticket, uint64_t *counts, uint64_t *num_ext, double *latency_ms,
+                           double timeout_ms) {
+    if (!sv) {
+        set_error("null server");
+        return KHZ_ERR_ARG;
+    }
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->results.find(ticket);
+    if (it == sv->results.end()) {
+        set_error("unknown ticket %llu", (unsigned long long)ticket);
+        return KHZ_ERR_NOT_FOUND;
+    }
+    const auto deadline = std::chrono::steady_clock::now() +
+                          std::chrono::microseconds((int64_t)(std::max(timeout_ms, 0.0) * 1000.0));
+    while (!sv->results[ticket].done) {
+        if (sv->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !sv->results[ticket].done) {
+            set_error("ticket %llu not finished within %.3f ms", (unsigned long long)ticket, timeout_ms);
+            return timeout_ms <= 0 ? KHZ_ERR_BUSY : KHZ_ERR_TIMEOUT;
+        }
+    }
+    ServeResult r = sv->results[ticket];
+    sv->results.erase(ticket);
+    if (r.status != KHZ_OK) {
+        set_error("query failed (status %d)", (int)r.status);
+        return r.status;
+    }
+    if (counts)
+        for (int c = 0; c < KHZ_MAX_COUNTS; ++c) counts[c] = r.counts[c];
+    if (num_ext) *num_ext = r.num_ext;
+    if (latency_ms) *latency_ms = r.latency_ms;
+    return KHZ_OK;
+}
+
+khz_status khz_server_stats_get(khz_server *sv, khz_server_stats *out) {
+    if (!sv || !out) {
+        set_error("null argument");
+        return KHZ_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(sv->mu);
+    memset(out, 0, sizeof(*out));
+    out->completed = sv->completed;
+    out->batches = sv->batches;
+    out->pending = sv->pending.size();
+    out->max_bytes_in_flight = sv->max_in_flight;
+    std::vector<double> l = sv->latencies;
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        out->p50_ms = l[(size_t)(0.50 * (l.size() - 1))];
+        out->p99_ms = l[(size_t)(0.99 * (l.size() - 1))];
+        out->max_ms = l.back();
+    }
+    if (sv->completed > 0 && sv->t_last > sv->t_first) out->queries_per_s = sv->completed / (sv->t_last - sv->t_first);
+    return KHZ_OK;
+}
+
+khz_status khz_server_reset_stats(khz_server *sv) {
+    if (!sv) return KHZ_ERR_ARG;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->latencies.clear();
+    sv->completed = 0;
+    sv->batches = 0;
+    sv->max_in_flight = sv->in_use;
+    sv->t_first = -1;
+    return KHZ_OK;
+}
+
+khz_status khz_server_destroy(khz_server *sv) {
+    if (!sv) return KHZ_OK;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+    }
+    sv->cv_work.notify_all();
+    if (sv->worker.joinable()) sv->worker.join();
+    cudaSetDevice(sv->ctx->device);
+    for (auto &sl : sv->slots) {
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
+        sl.plan.reset();
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.h_rows) cudaFreeHost(sl.h_rows);
+    }
+    delete sv;
     return KHZ_OK;
 }
 

@@ -45,7 +45,9 @@ EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_g
            "khz_graph_orient", "khz_graph_generate_rmat", "khz_graph_info_get", "khz_graph_export_csr",
            "khz_graph_write_dgraph", "khz_graph_free", "khz_count", "khz_count_async", "khz_app_num_counts",
            "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch", "khz_count_noalloc",
-           "khz_batch_create", "khz_batch_launch", "khz_batch_wait", "khz_batch_destroy"]
+           "khz_batch_create", "khz_batch_launch", "khz_batch_wait", "khz_batch_destroy",
+           "khz_server_create", "khz_server_submit", "khz_server_wait", "khz_server_stats_get",
+           "khz_server_reset_stats", "khz_server_destroy"]
 
 
 class KhzError(RuntimeError):
@@ -81,6 +83,15 @@ class Config(ctypes.Structure):
                 ("dfs_warps_per_sm", ctypes.c_int32), ("dfs_chunk", ctypes.c_int32),
                 ("bitmap_warp_max", ctypes.c_int32), ("bitmap_block_warps", ctypes.c_int32),
                 ("reserved", ctypes.c_int32 * 10)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("pending", ctypes.c_uint64),
+                ("max_bytes_in_flight", ctypes.c_uint64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("queries_per_s", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Job(ctypes.Structure):
@@ -126,6 +137,12 @@ def lib():
             "khz_batch_launch": (i32, [vp, vp]),
             "khz_batch_wait": (i32, [vp, P(u64), P(u64), vp]),
             "khz_batch_destroy": (i32, [vp]),
+            "khz_server_create": (i32, [vp, i32, i32, u64, P(vp)]),
+            "khz_server_submit": (i32, [vp, u32, i32, P(u64)]),
+            "khz_server_wait": (i32, [vp, u64, P(u64), P(u64), P(ctypes.c_double), ctypes.c_double]),
+            "khz_server_stats_get": (i32, [vp, P(ServerStats)]),
+            "khz_server_reset_stats": (i32, [vp]),
+            "khz_server_destroy": (i32, [vp]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -304,6 +321,41 @@ class Batch:
     def close(self):
         if self.ptr:
             lib().khz_batch_destroy(self.ptr)
+            self.ptr = None
+
+
+class Server:
+    """Continuous-batching counting server on device-resident graphs (native scheduler thread)."""
+
+    def __init__(self, ctx, slots=4, max_batch=64, hbm_budget=0):
+        p = ctypes.c_void_p()
+        _check(lib().khz_server_create(ctx.ptr, slots, max_batch, hbm_budget, ctypes.byref(p)))
+        self.ptr = p
+
+    def submit(self, graph, app):
+        t = ctypes.c_uint64(0)
+        _check(lib().khz_server_submit(self.ptr, graph.handle, _app_id(app), ctypes.byref(t)))
+        return t.value
+
+    def wait(self, ticket, app, timeout_ms=60000.0):
+        """-> (counts, NumExtensions, latency ms)"""
+        counts = (ctypes.c_uint64 * MAX_COUNTS)()
+        ext = ctypes.c_uint64(0)
+        lat = ctypes.c_double(0)
+        _check(lib().khz_server_wait(self.ptr, ticket, counts, ctypes.byref(ext), ctypes.byref(lat), timeout_ms))
+        return [int(counts[i]) for i in range(num_counts(app))], ext.value, lat.value
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib().khz_server_stats_get(self.ptr, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        _check(lib().khz_server_reset_stats(self.ptr))
+
+    def close(self):
+        if self.ptr:
+            lib().khz_server_destroy(self.ptr)
             self.ptr = None
 
 
