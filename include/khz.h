@@ -70,6 +70,7 @@ typedef uint32_t khz_graph; /* 0 is never a valid handle */
 #define KHZ_ENGINE_AUTO 0
 #define KHZ_ENGINE_DFS 1     /* per-warp DFS over the schedule with warp-cooperative set ops */
 #define KHZ_ENGINE_BITMAP 2  /* clique apps: local-subgraph bitmap engine on the oriented DAG */
+#define KHZ_ENGINE_WEDGE 3   /* 4-cycle app on symmetric graphs: wedge-endpoint counting */
 
 typedef struct khz_graph_info {
     uint32_t num_vertices;

@@ -114,9 +114,10 @@ struct BatchPlan {
     int rows = 0;
     std::vector<int> apps;
     bool stats = false;
-    bool has_bitmap = false, has_dfs = false;
+    bool has_bitmap = false, has_dfs = false, has_wedge = false;
     uint32_t engine = KHZ_ENGINE_DFS;
     BitmapLaunch bl;
+    WedgeLaunch wl;
     DfsLaunch dl;
     void *mem = nullptr;
     Arena arena;
@@ -266,11 +267,16 @@ khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
 
 // engine for one job under the context's configuration: the bitmap engine for clique apps on
 // graphs that are a DAG in id order or symmetric (oriented once, cached); the DFS engine otherwise
-int pick_engine(const khz_config &cfg, const AppDef &def, const Graph &g) {
+// and the wedge engine for the 4-cycle app on symmetric graphs.  Instrumented runs
+// (want_algo_bytes) of the 4-cycle use the DFS engine, which sums the schedule's set-op bytes.
+int pick_engine(const khz_config &cfg, const AppDef &def, int app, const Graph &g) {
+    const bool wedge_ok = app == KHZ_KGPI_4CYCLE && g.symmetric && !cfg.want_algo_bytes;
     int engine = cfg.engine;
-    if (engine == KHZ_ENGINE_AUTO) engine = def.clique ? KHZ_ENGINE_BITMAP : KHZ_ENGINE_DFS;
+    if (engine == KHZ_ENGINE_AUTO)
+        engine = def.clique ? KHZ_ENGINE_BITMAP : (wedge_ok ? KHZ_ENGINE_WEDGE : KHZ_ENGINE_DFS);
     if (engine == KHZ_ENGINE_BITMAP && !def.clique) engine = KHZ_ENGINE_DFS;
     if (engine == KHZ_ENGINE_BITMAP && !g.oriented && !g.symmetric) engine = KHZ_ENGINE_DFS;
+    if (engine == KHZ_ENGINE_WEDGE && !wedge_ok) engine = KHZ_ENGINE_DFS;
     return engine;
 }
 
@@ -298,12 +304,13 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     P->own_scratch = own_scratch;
     P->stats = ctx->cfg.want_algo_bytes != 0;
     std::vector<BJob> bjobs;
+    std::vector<WJob> wjobs;
     std::vector<DfsJob> djobs;
     std::vector<Plan> plans;
     std::vector<uint64_t> ext_add(n, 0);
     std::vector<uint32_t> mult((size_t)n * KHZ_MAX_COUNTS, 1);
     uint32_t bmax = 0, slot_cap = 32;
-    uint64_t vbase = 0, bm_entries = 0, unit_base = 0;
+    uint64_t vbase = 0, bm_entries = 0, unit_base = 0, wbase = 0;
     auto add_dfs = [&](const Graph &g, const Plan &pl, int row, uint32_t min_deg) {
         DfsJob j{};
         j.off = g.off;
@@ -323,7 +330,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         const AppDef &def = app_def(jobs[i].app);
         P->apps.push_back(jobs[i].app);
         for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
-        const int engine = pick_engine(ctx->cfg, def, *get_graph(ctx, jobs[i].graph));
+        const int engine = pick_engine(ctx->cfg, def, jobs[i].app, *get_graph(ctx, jobs[i].graph));
         if (engine == KHZ_ENGINE_BITMAP) {
             Graph *og = nullptr;
             khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
@@ -337,6 +344,12 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
                 add_dfs(*og, def.plans[0], i, bitmap_block_max_degree() + 1);
             ext_add[i] = og->n;
             P->engine = KHZ_ENGINE_BITMAP;
+        } else if (engine == KHZ_ENGINE_WEDGE) {
+            const Graph &g = *get_graph(ctx, jobs[i].graph);
+            wjobs.push_back(WJob{g.off, g.adj, g.n, 0, wbase, (uint32_t)i, 0});
+            wbase += g.n;
+            ext_add[i] = (uint64_t)g.n + g.m / 2;  // depth 0 and every undirected edge once at depth 1
+            if (P->engine == KHZ_ENGINE_DFS) P->engine = KHZ_ENGINE_WEDGE;
         } else {
             const Graph &g = *get_graph(ctx, jobs[i].graph);
             for (int r = 0; r < def.num_runs; ++r) add_dfs(g, def.plans[r], i, 0);
@@ -345,12 +358,16 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     }
     P->has_bitmap = !bjobs.empty();
     P->has_dfs = !djobs.empty();
+    P->has_wedge = !wjobs.empty();
+    uint32_t wmax_n = 0;
+    for (const auto &w : wjobs) wmax_n = std::max(wmax_n, w.n);
     const uint64_t list_cap = std::min<uint64_t>(std::max<uint64_t>(vbase, 1), bm_entries / 65 + 1);
     const uint64_t dfs_warps = dfs_total_warps(ctx->cfg.dfs_warps_per_sm);
     size_t bytes = 2 * Arena::round(sizeof(uint64_t) * kRowWords * n) + Arena::round(sizeof(uint32_t) * mult.size()) +
                    Arena::round(sizeof(uint64_t) * n) + Arena::round(sizeof(unsigned int)) +
                    Arena::round(sizeof(uint64_t) * kPhases);
     if (P->has_bitmap) bytes += bitmap_arena_bytes((int)bjobs.size(), list_cap);
+    if (P->has_wedge) bytes += wedge_arena_bytes((int)wjobs.size(), wbase, wedge_workers(wmax_n), wmax_n);
     if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
     P->slot_words = P->has_dfs ? dfs_slot_words(ctx->cfg.dfs_warps_per_sm, slot_cap) : 0;
     cudaError_t e;
@@ -381,6 +398,8 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     khz_status st = KHZ_OK;
     if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, &P->arena, &P->bl, s);
     if (st) return st;
+    if (P->has_wedge) st = wedge_prepare(wjobs, &P->arena, &P->wl, s);
+    if (st) return st;
     if (P->has_dfs)
         st = dfs_prepare(djobs, plans, slot_cap, ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, P->stats, own_scratch,
                          &P->arena, &P->dl, s);
@@ -409,6 +428,8 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
     if (ev_begin) KHZ_CUDA(cudaEventRecord(ev_begin, s));
     khz_status st = KHZ_OK;
     if (P->has_bitmap) st = bitmap_enqueue(P->bl, P->d_raw, s, ls);
+    if (st) return st;
+    if (P->has_wedge) st = wedge_enqueue(P->wl, P->d_raw, s, ls);
     if (st) return st;
     if (P->has_dfs) st = dfs_enqueue(P->dl, P->d_raw, s, ls, P->own_scratch ? nullptr : shared_slots);
     if (st) return st;
@@ -532,7 +553,10 @@ khz_status serve_footprint(khz_server *sv, khz_graph h, int app, uint64_t *bytes
     if (!g) return KHZ_ERR_ARG;
     const AppDef &def = app_def(app);
     uint64_t b = 1ull << 16;
-    if (pick_engine(ctx->cfg, def, *g) == KHZ_ENGINE_BITMAP) {
+    const int eng = pick_engine(ctx->cfg, def, app, *g);
+    if (eng == KHZ_ENGINE_WEDGE) {
+        b += 3 * 4 * (uint64_t)g->n + 4ull * wedge_workers(g->n) * g->n;
+    } else if (eng == KHZ_ENGINE_BITMAP) {
         Graph *og = nullptr;
         khz_status st = oriented_of(ctx, h, &og, nullptr);  // orient once, before any timing matters
         if (st) return st;
@@ -746,7 +770,7 @@ khz_status khz_ctx_set_config(khz_ctx *ctx, const khz_config *cfg) {
         set_error("null argument");
         return KHZ_ERR_ARG;
     }
-    if (cfg->engine < 0 || cfg->engine > KHZ_ENGINE_BITMAP) {
+    if (cfg->engine < 0 || cfg->engine > KHZ_ENGINE_WEDGE) {
         set_error("invalid engine %d", cfg->engine);
         return KHZ_ERR_ARG;
     }

@@ -141,6 +141,29 @@ struct BitmapLaunch {
     int block_threads[2] = {0, 0}, block_grid[2] = {0, 0}, block_dcap[2] = {0, 0};
 };
 
+// one (symmetric graph, 4-cycle app) job of a wedge-engine launch (global start-vertex index space)
+struct WJob {
+    const uint64_t *off;
+    const uint32_t *adj;
+    uint32_t n;
+    uint32_t pad;
+    uint64_t vbase;
+    uint32_t out_row;
+    uint32_t pad2;
+};
+
+struct WedgeLaunch {
+    const WJob *d_jobs = nullptr;
+    int n_jobs = 0;
+    uint64_t n_total = 0, list_cap = 0;
+    uint32_t max_n = 0;
+    uint32_t *lists = nullptr;   // warp, block and global tier lists (list_cap each)
+    unsigned int *cnt = nullptr;
+    unsigned long long *queues = nullptr;
+    uint32_t *dense = nullptr;   // workers * max_n counters, kept zeroed
+    int workers = 0, sms = 0;
+};
+
 // device resources and launch shape of one DFS-engine launch
 struct DfsLaunch {
     const DfsJob *d_jobs = nullptr;
@@ -215,6 +238,12 @@ khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_p
 // beyond depth 0 (row[6]) and, instrumented, the algorithmic bytes (row[7]).  Start vertices of
 // out-degree above bitmap_block_max_degree() are skipped: run them on the DFS engine with
 // DfsJob::min_deg.  No host synchronisation in bitmap_enqueue.
+// Wedge engine (4-cycle on symmetric graphs): adds each job's count (row[0]) and its level-2
+// NumExtensions (row[6]); no host synchronisation in wedge_enqueue.
+int wedge_workers(uint32_t max_n);
+size_t wedge_arena_bytes(int n_jobs, uint64_t n_total, int workers, uint32_t max_n);
+khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunch *wl, cudaStream_t s);
+khz_status wedge_enqueue(const WedgeLaunch &wl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap);
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
                           Arena *arena, BitmapLaunch *bl, cudaStream_t s);

@@ -1,0 +1,275 @@
+// Wedge engine for the 4-cycle app on symmetric graphs.
+//
+// The schedule (kgraphpi idiom: v1 > v0, v2 in N(v1) with v2 > v0, last level
+// |{v3 in N(v0) n N(v2) : v3 > v1}| minus matched vertices) intersects N(v0) with N(v2) once per
+// partial embedding (v0, v1, v2).  Grouped by (v0, v2) its count is C(c, 2) with
+// c = |{w in N(v0) n N(v2) : w > v0}|, so this engine enumerates every wedge (v0, w, v2) with
+// w > v0 and v2 > v0 exactly once and counts wedge endpoints v2 per start vertex.  An increment
+// that returns the previous count `old` adds `old` to the result: summed over a run of c increments
+// that is C(c, 2), so no second pass is needed.  The wedges enumerated are exactly the schedule's
+// level-2 embeddings, so NumExtensions = n + |E| + #wedges.
+//
+// Tiers by the number of wedges of v0 (an upper bound on distinct endpoints): one warp with a
+// 512-slot shared hash (<= 384 wedges), one block with an 8192-slot shared hash (<= 6144), or one
+// block with a dense counter array in global memory (reset by re-walking the wedges).
+#include <cuda_runtime.h>
+
+#include "khz_internal.cuh"
+#include "setops.cuh"
+
+namespace khz {
+namespace {
+
+constexpr uint32_t kEmptyKey = 0xffffffffu;
+constexpr int kWarpSlots = 512, kWarpWedges = 384;
+constexpr int kBlockSlots = 8192, kBlockWedges = 6144;
+constexpr int kBlockThreads = 512;
+
+__device__ __forceinline__ int wjob_of(const WJob *jobs, int n_jobs, uint64_t gv) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].vbase <= gv) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint64_t *wrow(uint64_t *rows, const WJob &j) { return rows + (size_t)j.out_row * kRowWords; }
+
+// add v2 to an open-addressing (key, count) table; returns the count before the increment
+__device__ __forceinline__ uint32_t hash_increment(uint32_t *keys, uint32_t *cnts, uint32_t mask, uint32_t v2) {
+    uint32_t h = (v2 * 0x9E3779B1u) & mask;
+    while (true) {
+        const uint32_t k = keys[h];
+        if (k == v2) return atomicAdd(&cnts[h], 1u);
+        if (k == kEmptyKey) {
+            const uint32_t prev = atomicCAS(&keys[h], kEmptyKey, v2);
+            if (prev == kEmptyKey || prev == v2) return atomicAdd(&cnts[h], 1u);
+        }
+        h = (h + 1) & mask;
+    }
+}
+
+// pass 1, one warp per start vertex: its wedge count (level-2 extensions) and its tier list
+__global__ void wedge_classify_kernel(const WJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
+                                      unsigned int *cnt, uint32_t *lists, uint64_t list_cap, uint64_t *rows) {
+    const unsigned lane = lane_id();
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t gv = warp; gv < n_total; gv += nwarps) {
+        const int j = wjob_of(jobs, n_jobs, gv);
+        const WJob &J = jobs[j];
+        const uint32_t v0 = (uint32_t)(gv - J.vbase);
+        const uint64_t b = J.off[v0], e = J.off[v0 + 1];
+        const uint32_t start = upper_bound_u32(J.adj + b, 0, (uint32_t)(e - b), v0);
+        uint64_t wedges = 0;
+        for (uint64_t i = b + start + lane; i < e; i += 32) {
+            const uint32_t w = J.adj[i];
+            const uint64_t wb = J.off[w], we = J.off[w + 1];
+            wedges += (we - wb) - upper_bound_u32(J.adj + wb, 0, (uint32_t)(we - wb), v0);
+        }
+        for (int o = 16; o > 0; o >>= 1) wedges += __shfl_down_sync(kFull, wedges, o);
+        if (lane == 0 && wedges > 0) {
+            atomicAdd((unsigned long long *)&wrow(rows, J)[KHZ_MAX_COUNTS], (unsigned long long)wedges);
+            const int t = wedges <= (uint64_t)kWarpWedges ? 0 : (wedges <= (uint64_t)kBlockWedges ? 1 : 2);
+            const unsigned int pos = atomicAdd(&cnt[t], 1u);
+            lists[(size_t)t * list_cap + pos] = (uint32_t)gv;
+        }
+    }
+}
+
+// Walk the wedges (v0, w, v2) of one start vertex with the calling threads: warp `wid` of `nw`
+// takes every nw-th w, its lanes take consecutive v2.  f(v2) is called once per wedge.
+template <typename F>
+__device__ __forceinline__ void walk_wedges(const WJob &J, uint32_t v0, int wid, int nw, F f) {
+    const unsigned lane = lane_id();
+    const uint64_t b = J.off[v0], e = J.off[v0 + 1];
+    const uint32_t start = upper_bound_u32(J.adj + b, 0, (uint32_t)(e - b), v0);
+    for (uint64_t i = b + start + wid; i < e; i += nw) {
+        const uint32_t w = J.adj[i];
+        const uint64_t wb = J.off[w], we = J.off[w + 1];
+        const uint32_t s2 = upper_bound_u32(J.adj + wb, 0, (uint32_t)(we - wb), v0);
+        for (uint64_t k = wb + s2 + lane; k < we; k += 32) f(__ldg(J.adj + k));
+    }
+}
+
+__device__ __forceinline__ void flush_count(uint64_t &acc, uint64_t *row) {
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+    if (lane_id() == 0 && acc) atomicAdd((unsigned long long *)&row[0], (unsigned long long)acc);
+    acc = 0;
+}
+
+__global__ void __launch_bounds__(256) wedge_warp_kernel(const WJob *__restrict__ jobs, int n_jobs,
+                                                         const uint32_t *__restrict__ list,
+                                                         const unsigned int *__restrict__ list_len,
+                                                         unsigned long long *queue, uint64_t *rows) {
+    __shared__ uint32_t s_keys[8][kWarpSlots];
+    __shared__ uint32_t s_cnts[8][kWarpSlots];
+    const unsigned lane = lane_id();
+    const int wib = threadIdx.x >> 5;
+    uint32_t *keys = s_keys[wib], *cnts = s_cnts[wib];
+    const unsigned int n_list = *list_len;
+    uint64_t acc = 0;
+    int cur = -1;
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(queue, 1ull);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= n_list) break;
+        const uint64_t gv = list[t];
+        const int j = wjob_of(jobs, n_jobs, gv);
+        if (j != cur) {
+            if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+            cur = j;
+        }
+        __syncwarp();
+        for (int k = lane; k < kWarpSlots; k += 32) {
+            keys[k] = kEmptyKey;
+            cnts[k] = 0;
+        }
+        __syncwarp();
+        walk_wedges(jobs[j], (uint32_t)(gv - jobs[j].vbase), 0, 1,
+                    [&](uint32_t v2) { acc += hash_increment(keys, cnts, kWarpSlots - 1, v2); });
+    }
+    if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+}
+
+__global__ void __launch_bounds__(kBlockThreads) wedge_block_kernel(const WJob *__restrict__ jobs, int n_jobs,
+                                                                    const uint32_t *__restrict__ list,
+                                                                    const unsigned int *__restrict__ list_len,
+                                                                    unsigned long long *queue, uint64_t *rows) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ uint64_t s_gv;
+    uint32_t *keys = smem, *cnts = smem + kBlockSlots;
+    const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned int n_list = *list_len;
+    uint64_t acc = 0;
+    int cur = -1;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(queue, 1ull);
+            s_gv = t < n_list ? list[t] : ~0ull;
+        }
+        __syncthreads();
+        const uint64_t gv = s_gv;
+        if (gv == ~0ull) break;
+        const int j = wjob_of(jobs, n_jobs, gv);
+        if (j != cur) {
+            if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+            cur = j;
+        }
+        for (int k = threadIdx.x; k < kBlockSlots; k += blockDim.x) {
+            keys[k] = kEmptyKey;
+            cnts[k] = 0;
+        }
+        __syncthreads();
+        walk_wedges(jobs[j], (uint32_t)(gv - jobs[j].vbase), wid, nw,
+                    [&](uint32_t v2) { acc += hash_increment(keys, cnts, kBlockSlots - 1, v2); });
+        __syncthreads();
+    }
+    if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+}
+
+// one block per heavy start vertex; `dense` holds one zeroed counter array of max_n words per
+// block, left zeroed after each start vertex by walking its wedges again
+__global__ void __launch_bounds__(kBlockThreads) wedge_global_kernel(const WJob *__restrict__ jobs, int n_jobs,
+                                                                     const uint32_t *__restrict__ list,
+                                                                     const unsigned int *__restrict__ list_len,
+                                                                     unsigned long long *queue, uint32_t *dense,
+                                                                     uint32_t max_n, uint64_t *rows) {
+    __shared__ uint64_t s_gv;
+    uint32_t *cnt = dense + (size_t)blockIdx.x * max_n;
+    const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned int n_list = *list_len;
+    uint64_t acc = 0;
+    int cur = -1;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const unsigned long long t = atomicAdd(queue, 1ull);
+            s_gv = t < n_list ? list[t] : ~0ull;
+        }
+        __syncthreads();
+        const uint64_t gv = s_gv;
+        if (gv == ~0ull) break;
+        const int j = wjob_of(jobs, n_jobs, gv);
+        if (j != cur) {
+            if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+            cur = j;
+        }
+        const uint32_t v0 = (uint32_t)(gv - jobs[j].vbase);
+        walk_wedges(jobs[j], v0, wid, nw, [&](uint32_t v2) { acc += atomicAdd(&cnt[v2], 1u); });
+        __syncthreads();
+        walk_wedges(jobs[j], v0, wid, nw, [&](uint32_t v2) { cnt[v2] = 0; });
+        __syncthreads();
+    }
+    if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+}
+
+}  // namespace
+
+size_t wedge_arena_bytes(int n_jobs, uint64_t n_total, int workers, uint32_t max_n) {
+    return Arena::round(sizeof(WJob) * (size_t)std::max(n_jobs, 1)) +
+           Arena::round(sizeof(uint32_t) * 3 * std::max<uint64_t>(n_total, 1)) + Arena::round(sizeof(unsigned int) * 8) +
+           Arena::round(sizeof(unsigned long long) * 4) + Arena::round(sizeof(uint32_t) * (size_t)workers * max_n);
+}
+
+int wedge_workers(uint32_t max_n) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // at most two blocks per SM, and at most ~1 GiB of dense counters
+    const uint64_t cap = (1ull << 30) / (4ull * std::max<uint32_t>(max_n, 1));
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)std::max(sms, 1) * 2, cap));
+}
+
+khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunch *wl, cudaStream_t s) {
+    WedgeLaunch L;
+    L.n_jobs = (int)jobs.size();
+    L.n_total = jobs.empty() ? 0 : jobs.back().vbase + jobs.back().n;
+    if (L.n_total >= (1ull << 32)) {
+        set_error("a wedge launch serves at most 2^32 - 1 start vertices");
+        return KHZ_ERR_ARG;
+    }
+    for (const auto &j : jobs) L.max_n = std::max(L.max_n, j.n);
+    L.workers = wedge_workers(L.max_n);
+    WJob *d_jobs = arena->take<WJob>(jobs.size());
+    L.lists = arena->take<uint32_t>(3 * std::max<uint64_t>(L.n_total, 1));
+    L.cnt = arena->take<unsigned int>(8);
+    L.queues = arena->take<unsigned long long>(4);
+    L.dense = arena->take<uint32_t>((size_t)L.workers * std::max<uint32_t>(L.max_n, 1));
+    if (!d_jobs || !L.lists || !L.cnt || !L.queues || !L.dense) {
+        set_error("wedge launch arena too small");
+        return KHZ_ERR_OOM;
+    }
+    L.list_cap = std::max<uint64_t>(L.n_total, 1);
+    if (!jobs.empty())
+        KHZ_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(WJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+    KHZ_CUDA(cudaMemsetAsync(L.dense, 0, sizeof(uint32_t) * (size_t)L.workers * std::max<uint32_t>(L.max_n, 1), s));
+    KHZ_CUDA(cudaFuncSetAttribute(wedge_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * kBlockSlots * sizeof(uint32_t))));
+    int dev = 0;
+    KHZ_CUDA(cudaGetDevice(&dev));
+    KHZ_CUDA(cudaDeviceGetAttribute(&L.sms, cudaDevAttrMultiProcessorCount, dev));
+    L.d_jobs = d_jobs;
+    *wl = L;
+    return KHZ_OK;
+}
+
+khz_status wedge_enqueue(const WedgeLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls) {
+    if (L.n_jobs == 0 || L.n_total == 0) return KHZ_OK;
+    KHZ_CUDA(cudaMemsetAsync(L.cnt, 0, sizeof(unsigned int) * 8, s));
+    KHZ_CUDA(cudaMemsetAsync(L.queues, 0, sizeof(unsigned long long) * 4, s));
+    const int cgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 7) / 8, (uint64_t)L.sms * 16));
+    wedge_classify_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.cnt, L.lists, L.list_cap, d_rows);
+    wedge_warp_kernel<<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.lists, L.cnt + 0, &L.queues[0], d_rows);
+    wedge_block_kernel<<<L.sms * 2, kBlockThreads, 2 * kBlockSlots * sizeof(uint32_t), s>>>(
+        L.d_jobs, L.n_jobs, L.lists + L.list_cap, L.cnt + 1, &L.queues[1], d_rows);
+    wedge_global_kernel<<<L.workers, kBlockThreads, 0, s>>>(L.d_jobs, L.n_jobs, L.lists + 2 * L.list_cap, L.cnt + 2,
+                                                           &L.queues[2], L.dense, std::max<uint32_t>(L.max_n, 1),
+                                                           d_rows);
+    KHZ_CUDA(cudaGetLastError());
+    if (ls) ls->launches += 4;
+    return KHZ_OK;
+}
+
+}  // namespace khz

@@ -30,7 +30,7 @@ EDGES_ON_DEVICE = 0x1
 ORIENT = 0x2
 UNCHECKED = 0x4
 
-ENGINE_AUTO, ENGINE_DFS, ENGINE_BITMAP = 0, 1, 2
+ENGINE_AUTO, ENGINE_DFS, ENGINE_BITMAP, ENGINE_WEDGE = 0, 1, 2, 3
 
 SETOP = {"intersect": 0, "subtract": 1, "intersect_count": 2, "bounded_intersect": 3,
          "bounded_subtract": 4, "trim": 5, "trim_lower_bound": 6}

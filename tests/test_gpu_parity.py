@@ -355,3 +355,30 @@ def test_bitmap_overflow_tier_complete_graph(khz_ctx):
     finally:
         khz_ctx.set_config(engine=khz.ENGINE_AUTO)
         g.free()
+
+
+def test_wedge_engine_matches_dfs_engine(khz_ctx):
+    """4-cycle on a skewed R-MAT (hub start vertices reach the global-memory tier): the wedge
+    engine and the DFS engine (the schedule as written) agree on counts and NumExtensions."""
+    from openkhuzdulgraph_b200 import khz
+    g = khz_ctx.generate_rmat(14, 16, seed=4)
+    try:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+        w, sw = khz_ctx.count(g, "kgraphpi_four_cycle")
+        assert sw.engine == khz.ENGINE_WEDGE
+        khz_ctx.set_config(engine=khz.ENGINE_DFS)
+        d, sd = khz_ctx.count(g, "kgraphpi_four_cycle")
+        assert w == d and sw.num_extensions == sd.num_extensions
+        # and on a small graph against the oracle
+        canon, n = orc.rmat(11, 16, seed=6)
+        sym = orc.symmetrize(canon)
+        off, adj = orc.csr(sym, n)
+        g2 = khz_ctx.graph_from_edges(sym, n)
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+        got, st = khz_ctx.count(g2, "kgraphpi_four_cycle")
+        exp, ext, _ = orc.count("kgraphpi_four_cycle", off, adj)
+        assert got == exp and st.num_extensions == ext
+        g2.free()
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+        g.free()
