@@ -56,6 +56,38 @@ __global__ void finalize_kernel(const uint64_t *raw, int rows, const uint32_t *m
     out[(size_t)r * kRowWords + KHZ_MAX_COUNTS + 1] = raw[(size_t)r * kRowWords + KHZ_MAX_COUNTS + 1];
 }
 
+// 3-motif jobs counted from their triangle count: one block per job sums C(d, 2) over the
+// symmetric graph and writes the wedge counter of its raw row (after the triangle launches):
+//   kautomine (vertex-induced, multiplicity 2): raw = 2 * (sum C(d,2) - 3 T)
+//   kgraphpi (edge-induced): sum C(d,2)
+struct MJob {
+    const uint64_t *off;
+    uint32_t n;
+    uint32_t out_row;
+    int32_t vertex_induced;
+    int32_t pad;
+};
+
+__global__ void motif3_combine_kernel(const MJob *__restrict__ jobs, uint64_t *rows) {
+    const MJob J = jobs[blockIdx.x];
+    __shared__ unsigned long long s_sum;
+    if (threadIdx.x == 0) s_sum = 0;
+    __syncthreads();
+    unsigned long long part = 0;
+    for (uint32_t v = threadIdx.x; v < J.n; v += blockDim.x) {
+        const unsigned long long d = J.off[v + 1] - J.off[v];
+        part += d * (d - (d > 0 ? 1 : 0)) / 2;
+    }
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_sum, part);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t *row = rows + (size_t)J.out_row * kRowWords;
+        const uint64_t t = row[0];
+        row[1] = J.vertex_induced ? 2 * (s_sum - 3 * t) : s_sum;
+    }
+}
+
 // VertexSet ops as a batch: one warp per pair (vertex_set.cc:20-184, utilities.h:64-86)
 __global__ void setop_batch_kernel(int op, const uint64_t *a_off, const uint32_t *a, const uint64_t *b_off,
                                    const uint32_t *b, const uint32_t *bound, uint32_t *out, uint32_t *out_len,
@@ -115,6 +147,8 @@ struct BatchPlan {
     std::vector<int> apps;
     bool stats = false;
     bool has_bitmap = false, has_dfs = false, has_wedge = false;
+    MJob *d_mjobs = nullptr;
+    int n_mjobs = 0;
     uint32_t engine = KHZ_ENGINE_DFS;
     BitmapLaunch bl;
     WedgeLaunch wl;
@@ -271,9 +305,11 @@ khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
 // (want_algo_bytes) of the 4-cycle use the DFS engine, which sums the schedule's set-op bytes.
 int pick_engine(const khz_config &cfg, const AppDef &def, int app, const Graph &g) {
     const bool wedge_ok = app == KHZ_KGPI_4CYCLE && g.symmetric && !cfg.want_algo_bytes;
+    const bool motif3 = (app == KHZ_KAUTO_3MOTIF || app == KHZ_KGPI_3MOTIF) && g.symmetric && !cfg.want_algo_bytes;
     int engine = cfg.engine;
     if (engine == KHZ_ENGINE_AUTO)
-        engine = def.clique ? KHZ_ENGINE_BITMAP : (wedge_ok ? KHZ_ENGINE_WEDGE : KHZ_ENGINE_DFS);
+        engine = def.clique || motif3 ? KHZ_ENGINE_BITMAP : (wedge_ok ? KHZ_ENGINE_WEDGE : KHZ_ENGINE_DFS);
+    if (engine == KHZ_ENGINE_BITMAP && motif3) return KHZ_ENGINE_BITMAP;
     if (engine == KHZ_ENGINE_BITMAP && !def.clique) engine = KHZ_ENGINE_DFS;
     if (engine == KHZ_ENGINE_BITMAP && !g.oriented && !g.symmetric) engine = KHZ_ENGINE_DFS;
     if (engine == KHZ_ENGINE_WEDGE && !wedge_ok) engine = KHZ_ENGINE_DFS;
@@ -304,6 +340,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     P->own_scratch = own_scratch;
     P->stats = ctx->cfg.want_algo_bytes != 0;
     std::vector<BJob> bjobs;
+    std::vector<MJob> mjobs;
     std::vector<WJob> wjobs;
     std::vector<DfsJob> djobs;
     std::vector<Plan> plans;
@@ -331,7 +368,25 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         P->apps.push_back(jobs[i].app);
         for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
         const int engine = pick_engine(ctx->cfg, def, jobs[i].app, *get_graph(ctx, jobs[i].graph));
-        if (engine == KHZ_ENGINE_BITMAP) {
+        if (engine == KHZ_ENGINE_BITMAP && !def.clique) {
+            // 3-motif: triangles on the oriented view (bitmap engine, k = 3) + degree sums
+            const Graph sg = *get_graph(ctx, jobs[i].graph);
+            Graph *og = nullptr;
+            khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
+            if (st) return st;
+            bjobs.push_back(BJob{og->off, og->adj, og->n, 3, vbase, (uint32_t)i, 0});
+            vbase += og->n;
+            bm_entries += og->m;
+            bmax = std::max(bmax, og->max_degree);
+            if (og->max_degree > bitmap_block_max_degree())
+                add_dfs(*og, app_def(KHZ_KAUTO_TRIANGLE).plans[0], i, bitmap_block_max_degree() + 1);
+            const bool kauto = jobs[i].app == KHZ_KAUTO_3MOTIF;
+            mjobs.push_back(MJob{sg.off, sg.n, (uint32_t)i, kauto ? 1 : 0, 0});
+            // the bitmap launch adds one level-1 extension per undirected edge; kautomine's fused run
+            // extends every (v0, v1) pair (twice that), kgraphpi's wedge run adds only its start vertices
+            ext_add[i] = kauto ? (uint64_t)sg.n + sg.m / 2 : 2ull * sg.n;
+            P->engine = KHZ_ENGINE_BITMAP;
+        } else if (engine == KHZ_ENGINE_BITMAP) {
             Graph *og = nullptr;
             khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
             if (st) return st;
@@ -368,6 +423,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
                    Arena::round(sizeof(uint64_t) * kPhases);
     if (P->has_bitmap) bytes += bitmap_arena_bytes((int)bjobs.size(), list_cap);
     if (P->has_wedge) bytes += wedge_arena_bytes((int)wjobs.size(), wbase, wedge_workers(wmax_n), wmax_n);
+    if (!mjobs.empty()) bytes += Arena::round(sizeof(MJob) * mjobs.size());
     if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
     P->slot_words = P->has_dfs ? dfs_slot_words(ctx->cfg.dfs_warps_per_sm, slot_cap) : 0;
     cudaError_t e;
@@ -400,6 +456,11 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     if (st) return st;
     if (P->has_wedge) st = wedge_prepare(wjobs, &P->arena, &P->wl, s);
     if (st) return st;
+    if (!mjobs.empty()) {
+        P->d_mjobs = P->arena.take<MJob>(mjobs.size());
+        P->n_mjobs = (int)mjobs.size();
+        KHZ_CUDA(cudaMemcpyAsync(P->d_mjobs, mjobs.data(), sizeof(MJob) * mjobs.size(), cudaMemcpyHostToDevice, s));
+    }
     if (P->has_dfs)
         st = dfs_prepare(djobs, plans, slot_cap, ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, P->stats, own_scratch,
                          &P->arena, &P->dl, s);
@@ -429,9 +490,14 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
     khz_status st = KHZ_OK;
     if (P->has_bitmap) st = bitmap_enqueue(P->bl, P->d_raw, s, ls);
     if (st) return st;
-    if (P->has_wedge) st = wedge_enqueue(P->wl, P->d_raw, s, ls);
-    if (st) return st;
     if (P->has_dfs) st = dfs_enqueue(P->dl, P->d_raw, s, ls, P->own_scratch ? nullptr : shared_slots);
+    if (st) return st;
+    if (P->n_mjobs) {  // after every launch that counts triangles
+        motif3_combine_kernel<<<P->n_mjobs, 256, 0, s>>>(P->d_mjobs, P->d_raw);
+        KHZ_CUDA(cudaGetLastError());
+        if (ls) ls->launches += 1;
+    }
+    if (P->has_wedge) st = wedge_enqueue(P->wl, P->d_raw, s, ls);
     if (st) return st;
     if (ev_end) KHZ_CUDA(cudaEventRecord(ev_end, s));
     finalize_kernel<<<(unsigned)((P->rows + 127) / 128), 128, 0, s>>>(P->d_raw, P->rows, P->d_mult, P->d_extadd,
