@@ -17,6 +17,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libkhz_b200.so")
+APP = os.path.join(HERE, "khz_app")
+HOST_CXX = os.environ.get("KHZ_HOST_CXX", "g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,6 +50,15 @@ def build(verbose=False, ptxas_verbose=False):
             f.result()
     if _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    # the reference-style command-line program over the C ABI (host C++ only)
+    app_src = os.path.join(HERE, "host", "khz_app.cpp")
+    hpp = os.path.join(ROOT, "include", "khz_khuzdul.hpp")
+    if _newer(APP, [app_src, hpp, LIB]):
+        cmd = [HOST_CXX, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), app_src, "-o", APP,
+               "-L" + HERE, "-lkhz_b200", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
