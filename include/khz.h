@@ -179,6 +179,21 @@ khz_status khz_batch_launch(khz_batch *batch, void *stream);
 khz_status khz_batch_wait(khz_batch *batch, uint64_t *counts, uint64_t *num_ext, void *stream);
 khz_status khz_batch_destroy(khz_batch *batch);
 
+/* ---- autotuner ---------------------------------------------------------------------- */
+/* Times the given jobs (a representative sample of the workload) under candidate settings —
+ * engine (the bitmap / wedge / identity engines vs the DFS engine's warp-cooperative binary-search
+ * probes), DFS warps per SM {8, 16, 32}, DFS units per grab {2, 8, 32}, bitmap warp-tier degree
+ * threshold {32, 64} — by coordinate descent (two passes, best of `reps` each), checks that every
+ * candidate produces the same counts, and installs the fastest in the context. */
+typedef struct khz_tune_report {
+    int32_t trials;
+    int32_t reserved;
+    double baseline_ms; /* the context's settings on entry */
+    double best_ms;
+    khz_config best;    /* now the context's configuration */
+} khz_tune_report;
+khz_status khz_autotune(khz_ctx *ctx, const khz_job *jobs, int n_jobs, int reps, khz_tune_report *report);
+
 /* ---- serving: continuous batching of counting queries ----------------------------- */
 /* A server owns `slots` CUDA streams and a scheduler thread.  Queries (graph, app) are admitted in
  * arrival order as slots and HBM budget free up (a query's footprint is its engine scratch: DFS

@@ -253,7 +253,7 @@ __device__ __forceinline__ uint64_t *row_of(uint64_t *rows, const BJob &j) { ret
 constexpr int kWarpHashLog = 7;  // 128-slot table per warp
 template <bool STATS>
 __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict__ jobs, int n_jobs,
-                                                          uint64_t n_total, uint32_t dmin,
+                                                          uint64_t n_total, uint32_t dmin, uint32_t warp_max,
                                                           unsigned long long *queue, uint64_t *rows_out,
                                                           uint64_t *phase_bytes) {
     constexpr int W = kWarpMax / 32;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict
             myv = (uint32_t)(gv - jobs[myj].vbase);
             myd = odeg(jobs[myj].off, myv);
         }
-        unsigned todo = __ballot_sync(kFull, myc < c1 && myd >= dmin && myd <= (uint32_t)kWarpMax);
+        unsigned todo = __ballot_sync(kFull, myc < c1 && myd >= dmin && myd <= warp_max);
         while (todo) {
             const int src = __ffs(todo) - 1;
             todo &= todo - 1;
@@ -407,8 +407,8 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
 //   mid list   = (128, 256] then (64, 128]
 //   large list = (1024, kBlockMax] then (512, 1024] then (256, 512]
 // Bucket 5 = overflow (left to the DFS engine), -1 = warp tier.
-__device__ __forceinline__ int bucket_of(uint32_t d) {
-    if (d <= (uint32_t)kWarpMax) return -1;
+__device__ __forceinline__ int bucket_of(uint32_t d, uint32_t warp_max) {
+    if (d <= warp_max) return -1;
     if (d <= 128) return 0;
     if (d <= (uint32_t)kMidMax) return 1;
     if (d <= 512) return 2;
@@ -424,7 +424,7 @@ constexpr int kCntCursor = 6, kCntBase = 12, kCntMidLen = 18, kCntLargeLen = 19;
 // pass 1: bucket sizes, and the level-1 extensions (v0, v1) of every start vertex this engine
 // serves (the reference counts one extension per scattered v1, engine.cc:924)
 __global__ void classify_count_kernel(const BJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
-                                      unsigned int *cnt, uint64_t *rows_out) {
+                                      uint32_t warp_max, unsigned int *cnt, uint64_t *rows_out) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: whole warps iterate together
     for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < ((n_total + 31) & ~31ull);
          gv += stride) {
@@ -433,7 +433,7 @@ __global__ void classify_count_kernel(const BJob *__restrict__ jobs, int n_jobs,
         if (gv < n_total) {
             j = job_of(jobs, n_jobs, gv);
             d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
-            b = bucket_of(d);
+            b = bucket_of(d, warp_max);
         }
         if (b >= 0 && b < 5) atomicAdd(&cnt[b], 1u);
         // one atomic per distinct job per warp
@@ -462,12 +462,13 @@ __global__ void classify_prefix_kernel(unsigned int *cnt) {
 
 // pass 2: write each block-tier start vertex into its list
 __global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
-                                      unsigned int *cnt, uint32_t *mid_list, uint32_t *large_list) {
+                                      uint32_t warp_max, unsigned int *cnt, uint32_t *mid_list,
+                                      uint32_t *large_list) {
     for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < n_total;
          gv += (uint64_t)gridDim.x * blockDim.x) {
         const int j = job_of(jobs, n_jobs, gv);
         const uint32_t d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
-        const int b = bucket_of(d);
+        const int b = bucket_of(d, warp_max);
         if (b < 0 || b >= 5) continue;
         const unsigned int pos = cnt[kCntBase + b] + atomicAdd(&cnt[kCntCursor + b], 1u);
         if (b <= 1) mid_list[pos] = (uint32_t)gv;
@@ -486,8 +487,9 @@ size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap) {
 }
 
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
-                          Arena *arena, BitmapLaunch *bl, cudaStream_t s) {
+                          int warp_max, Arena *arena, BitmapLaunch *bl, cudaStream_t s) {
     BitmapLaunch L;
+    L.warp_max = warp_max == 32 ? 32u : (uint32_t)kWarpMax;
     L.n_jobs = (int)jobs.size();
     L.n_total = jobs.empty() ? 0 : jobs.back().vbase + jobs.back().n;
     L.stats = stats;
@@ -511,7 +513,7 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     KHZ_CUDA(cudaGetDevice(&dev));
     KHZ_CUDA(cudaDeviceGetAttribute(&L.sms, cudaDevAttrMultiProcessorCount, dev));
     L.large_dcap = (int)std::min<uint32_t>((uint32_t)kBlockMax, std::max<uint32_t>(max_outdeg, kMidMax + 1));
-    L.has_mid = max_outdeg > (uint32_t)kWarpMax;
+    L.has_mid = max_outdeg > L.warp_max;
     L.has_large = max_outdeg > (uint32_t)kMidMax;
     const int dcaps[2] = {kMidMax, L.large_dcap};
     const int threads[2] = {256, 1024};
@@ -546,20 +548,21 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
     KHZ_CUDA(cudaMemsetAsync(L.cnt, 0, sizeof(unsigned int) * 32, s));
     KHZ_CUDA(cudaMemsetAsync(L.queues, 0, sizeof(unsigned long long) * 4, s));
     const int cgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 255) / 256, (uint64_t)L.sms * 8));
-    classify_count_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.cnt, d_rows);
+    classify_count_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, d_rows);
     if (L.has_mid) {
         classify_prefix_kernel<<<1, 32, 0, s>>>(L.cnt);
-        classify_write_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.cnt, L.mid_list, L.large_list);
+        classify_write_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, L.mid_list,
+                                                    L.large_list);
     }
     KHZ_CUDA(cudaGetLastError());
     if (ls) ls->launches += L.has_mid ? 3 : 1;
     mark(0, true);
     if (L.stats)
-        clique_warp_kernel<true><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 1u, &L.queues[0], d_rows,
-                                                           pb(0));
+        clique_warp_kernel<true><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 1u, L.warp_max,
+                                                           &L.queues[0], d_rows, pb(0));
     else
-        clique_warp_kernel<false><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 2u, &L.queues[0], d_rows,
-                                                            pb(0));
+        clique_warp_kernel<false><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 2u, L.warp_max,
+                                                            &L.queues[0], d_rows, pb(0));
     KHZ_CUDA(cudaGetLastError());
     mark(0, false);
     if (ls) ls->launches += 1;

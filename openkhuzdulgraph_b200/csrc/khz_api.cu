@@ -416,7 +416,9 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     P->has_wedge = !wjobs.empty();
     uint32_t wmax_n = 0;
     for (const auto &w : wjobs) wmax_n = std::max(wmax_n, w.n);
-    const uint64_t list_cap = std::min<uint64_t>(std::max<uint64_t>(vbase, 1), bm_entries / 65 + 1);
+    const int warp_max = ctx->cfg.bitmap_warp_max == 32 ? 32 : 64;
+    // every listed start vertex has more than warp_max out-edges
+    const uint64_t list_cap = std::min<uint64_t>(std::max<uint64_t>(vbase, 1), bm_entries / (warp_max + 1) + 1);
     const uint64_t dfs_warps = dfs_total_warps(ctx->cfg.dfs_warps_per_sm);
     size_t bytes = 2 * Arena::round(sizeof(uint64_t) * kRowWords * n) + Arena::round(sizeof(uint32_t) * mult.size()) +
                    Arena::round(sizeof(uint64_t) * n) + Arena::round(sizeof(unsigned int)) +
@@ -452,7 +454,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     KHZ_CUDA(cudaMemcpyAsync(P->d_mult, mult.data(), sizeof(uint32_t) * mult.size(), cudaMemcpyHostToDevice, s));
     KHZ_CUDA(cudaMemcpyAsync(P->d_extadd, ext_add.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
     khz_status st = KHZ_OK;
-    if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, &P->arena, &P->bl, s);
+    if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, warp_max, &P->arena, &P->bl, s);
     if (st) return st;
     if (P->has_wedge) st = wedge_prepare(wjobs, &P->arena, &P->wl, s);
     if (st) return st;
@@ -556,8 +558,8 @@ khz_status fill_stats(khz_ctx *ctx, BatchPlan *P, const LaunchStats &ls, bool ti
 // the cached prepared launch of one (graph, app) under the current configuration
 khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, BatchPlan **out) {
     char key[160];
-    snprintf(key, sizeof(key), "%u/%d/%d/%d/%d/%d", g, app, ctx->cfg.engine, ctx->cfg.want_algo_bytes,
-             ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk);
+    snprintf(key, sizeof(key), "%u/%d/%d/%d/%d/%d/%d", g, app, ctx->cfg.engine, ctx->cfg.want_algo_bytes,
+             ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, ctx->cfg.bitmap_warp_max);
     auto it = ctx->plans.find(key);
     if (it != ctx->plans.end()) {
         *out = it->second.get();
@@ -626,7 +628,7 @@ khz_status serve_footprint(khz_server *sv, khz_graph h, int app, uint64_t *bytes
         Graph *og = nullptr;
         khz_status st = oriented_of(ctx, h, &og, nullptr);  // orient once, before any timing matters
         if (st) return st;
-        b += 2 * 4 * (og->m / 65 + 1);
+        b += 2 * 4 * (og->m / 33 + 1);
         if (og->max_degree > bitmap_block_max_degree())
             b += 4 * dfs_slot_words(ctx->cfg.dfs_warps_per_sm, og->max_degree);
     } else {
@@ -842,6 +844,7 @@ khz_status khz_ctx_set_config(khz_ctx *ctx, const khz_config *cfg) {
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cfg = *cfg;
+    ctx->plans.clear();  // prepared launches of the previous configuration
     if (ctx->cfg.dfs_warps_per_sm <= 0) ctx->cfg.dfs_warps_per_sm = 16;
     if (ctx->cfg.dfs_chunk <= 0) ctx->cfg.dfs_chunk = 8;
     return KHZ_OK;
@@ -1397,6 +1400,93 @@ khz_status khz_server_destroy(khz_server *sv) {
         if (sl.h_rows) cudaFreeHost(sl.h_rows);
     }
     delete sv;
+    return KHZ_OK;
+}
+
+
+khz_status khz_autotune(khz_ctx *ctx, const khz_job *jobs, int n_jobs, int reps, khz_tune_report *report) {
+    khz_status st = check_ctx(ctx);
+    if (st) return st;
+    if (!jobs || n_jobs <= 0) {
+        set_error("empty job list");
+        return KHZ_ERR_ARG;
+    }
+    if (reps < 1) reps = 1;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const khz_config base = ctx->cfg;
+    cudaStream_t s = nullptr;
+    KHZ_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    std::vector<uint64_t> ref;
+    int trials = 0;
+    // one measurement: prepare the launch under `c`, run it once to warm, then best of `reps`
+    auto measure = [&](const khz_config &c, double *ms) -> khz_status {
+        ctx->cfg = c;
+        ctx->cfg.want_algo_bytes = 0;
+        std::unique_ptr<BatchPlan> P;
+        khz_status e = build_plan(ctx, jobs, n_jobs, s, kPlanOwnSlots | kPlanPinned, &P);
+        if (e) return e;
+        double best = 1e300;
+        for (int r = 0; r <= reps; ++r) {
+            e = enqueue_plan(P.get(), s, nullptr, ctx->ev0, ctx->ev1);
+            if (e) return e;
+            e = read_plan(P.get(), s);
+            if (e) return e;
+            float f = 0;
+            KHZ_CUDA(cudaEventElapsedTime(&f, ctx->ev0, ctx->ev1));
+            if (r > 0) best = std::min(best, (double)f);
+        }
+        std::vector<uint64_t> rows;
+        for (int i = 0; i < n_jobs; ++i)
+            for (int c2 = 0; c2 <= KHZ_MAX_COUNTS; ++c2) rows.push_back(P->h_final[(size_t)i * kRowWords + c2]);
+        if (ref.empty()) ref = rows;
+        else if (rows != ref) {
+            set_error("autotuner: candidate configurations disagree on the counts");
+            return KHZ_ERR_OVERFLOW;
+        }
+        ++trials;
+        *ms = best;
+        return KHZ_OK;
+    };
+    khz_config best = base;
+    best.want_algo_bytes = 0;
+    double best_ms = 0, base_ms = 0;
+    st = measure(best, &base_ms);
+    best_ms = base_ms;
+    // coordinate descent over the knobs, each from the current best
+    const int engines[] = {KHZ_ENGINE_AUTO, KHZ_ENGINE_DFS};
+    const int warps[] = {8, 16, 32};
+    const int chunks[] = {2, 8, 32};
+    const int warp_max[] = {32, 64};
+    for (int pass = 0; pass < 2 && st == KHZ_OK; ++pass) {
+        for (int knob = 0; knob < 4 && st == KHZ_OK; ++knob) {
+            const int *vals = knob == 0 ? engines : knob == 1 ? warps : knob == 2 ? chunks : warp_max;
+            const int nv = knob == 0 ? 2 : knob == 1 ? 3 : knob == 2 ? 3 : 2;
+            for (int v = 0; v < nv && st == KHZ_OK; ++v) {
+                khz_config c = best;
+                int *field = knob == 0 ? &c.engine : knob == 1 ? &c.dfs_warps_per_sm : knob == 2 ? &c.dfs_chunk
+                                                                                                 : &c.bitmap_warp_max;
+                if (*field == vals[v]) continue;
+                *field = vals[v];
+                double ms = 0;
+                st = measure(c, &ms);
+                if (st == KHZ_OK && ms < best_ms) {
+                    best_ms = ms;
+                    best = c;
+                }
+            }
+        }
+    }
+    cudaStreamDestroy(s);
+    ctx->cfg = st == KHZ_OK ? best : base;
+    ctx->cfg.want_algo_bytes = base.want_algo_bytes;
+    ctx->plans.clear();
+    if (st) return st;
+    if (report) {
+        report->trials = trials;
+        report->baseline_ms = base_ms;
+        report->best_ms = best_ms;
+        report->best = ctx->cfg;
+    }
     return KHZ_OK;
 }
 

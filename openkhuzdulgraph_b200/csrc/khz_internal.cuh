@@ -135,6 +135,7 @@ struct BitmapLaunch {
     unsigned int *cnt = nullptr;
     unsigned long long *queues = nullptr;
     int large_dcap = 0;
+    uint32_t warp_max = 64;  // out-degrees served by one warp (32 or 64)
     bool has_mid = false, has_large = false, stats = false;
     int sms = 0;
     size_t block_smem[2] = {0, 0};
@@ -246,7 +247,7 @@ khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunc
 khz_status wedge_enqueue(const WedgeLaunch &wl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap);
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
-                          Arena *arena, BitmapLaunch *bl, cudaStream_t s);
+                          int warp_max, Arena *arena, BitmapLaunch *bl, cudaStream_t s);
 khz_status bitmap_enqueue(const BitmapLaunch &bl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 uint32_t bitmap_block_max_degree();
 

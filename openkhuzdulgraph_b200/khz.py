@@ -47,7 +47,7 @@ EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_g
            "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch", "khz_count_noalloc",
            "khz_batch_create", "khz_batch_launch", "khz_batch_wait", "khz_batch_destroy",
            "khz_server_create", "khz_server_submit", "khz_server_wait", "khz_server_stats_get",
-           "khz_server_reset_stats", "khz_server_destroy"]
+           "khz_server_reset_stats", "khz_server_destroy", "khz_autotune"]
 
 
 class KhzError(RuntimeError):
@@ -92,6 +92,11 @@ class ServerStats(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("trials", ctypes.c_int32), ("reserved", ctypes.c_int32), ("baseline_ms", ctypes.c_double),
+                ("best_ms", ctypes.c_double), ("best", Config)]
 
 
 class Job(ctypes.Structure):
@@ -143,6 +148,7 @@ def lib():
             "khz_server_stats_get": (i32, [vp, P(ServerStats)]),
             "khz_server_reset_stats": (i32, [vp]),
             "khz_server_destroy": (i32, [vp]),
+            "khz_autotune": (i32, [vp, P(Job), i32, i32, P(TuneReport)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -275,6 +281,19 @@ class Context:
 
     def count_async(self, graph, app, d_out_ptr, stream=None):
         _check(lib().khz_count_async(self.ptr, graph.handle, _app_id(app), d_out_ptr, stream))
+
+    def autotune(self, jobs, reps=2):
+        """jobs: list of (Graph, app); installs the fastest settings -> report dict"""
+        arr = (Job * len(jobs))()
+        for i, (g, app) in enumerate(jobs):
+            arr[i].graph = g.handle
+            arr[i].app = _app_id(app)
+        rep = TuneReport()
+        _check(lib().khz_autotune(self.ptr, arr, len(jobs), reps, ctypes.byref(rep)))
+        b = rep.best
+        return {"trials": rep.trials, "baseline_ms": rep.baseline_ms, "best_ms": rep.best_ms,
+                "engine": b.engine, "dfs_warps_per_sm": b.dfs_warps_per_sm, "dfs_chunk": b.dfs_chunk,
+                "bitmap_warp_max": b.bitmap_warp_max}
 
     def count_batch(self, jobs, stream=None):
         """jobs: list of (Graph, app) -> (list of count lists, list of NumExtensions, Stats)"""

@@ -382,3 +382,18 @@ def test_wedge_engine_matches_dfs_engine(khz_ctx):
     finally:
         khz_ctx.set_config(engine=khz.ENGINE_AUTO)
         g.free()
+
+
+def test_autotuner_keeps_counts_and_installs_settings(graphs, khz_ctx):
+    from openkhuzdulgraph_b200 import khz
+    jobs = [(g, app) for spec, n, sym, off, adj, g in graphs[:4]
+            for app in ["kautomine_four_clique", "kgraphpi_four_cycle", "kautomine_four_motif"]]
+    expect = [khz_ctx.count(g, app)[0] for g, app in jobs]
+    rep = khz_ctx.autotune(jobs, reps=1)
+    try:
+        assert rep["trials"] >= 5 and rep["best_ms"] <= rep["baseline_ms"]
+        cfg = khz_ctx.config()
+        assert cfg.engine == rep["engine"] and cfg.dfs_chunk == rep["dfs_chunk"]
+        assert [khz_ctx.count(g, app)[0] for g, app in jobs] == expect
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO, dfs_warps_per_sm=16, dfs_chunk=8, bitmap_warp_max=64)
