@@ -212,6 +212,7 @@ struct ServeRequest {
     int app;
     double t_submit;  // seconds, steady clock
     uint64_t footprint;
+    int size_class;   // floor(log2(CSR entries + 1)): queries share a launch only within a class
 };
 
 struct ServeResult {
@@ -685,14 +686,22 @@ void serve_dispatch(khz_server *sv) {
         uint64_t fp = 0;
         {
             std::lock_guard<std::mutex> lk(sv->mu);
-            while (!sv->pending.empty() && (int)take.size() < sv->max_batch) {
-                const ServeRequest &r = sv->pending.front();
+            // the oldest query decides the size class of this launch; younger queries of the same
+            // class join it (so a large query does not hold small ones back, and small ones batch)
+            int cls = -1;
+            for (auto it = sv->pending.begin(); it != sv->pending.end() && (int)take.size() < sv->max_batch;) {
+                const ServeRequest &r = *it;
+                if (cls >= 0 && r.size_class != cls) {
+                    ++it;
+                    continue;
+                }
                 const bool fits = sv->in_use + fp + r.footprint <= sv->budget;
                 // a query larger than the whole budget still runs, alone, when nothing else does
                 if (!fits && !(take.empty() && sv->in_use == 0)) break;
+                cls = r.size_class;
                 fp += r.footprint;
                 take.push_back(r);
-                sv->pending.pop_front();
+                it = sv->pending.erase(it);
             }
             if (take.empty()) return;
             sv->in_use += fp;
@@ -1304,11 +1313,18 @@ khz_status khz_server_submit(khz_server *sv, khz_graph g, khz_app_id app, khz_ti
     }
     st = serve_footprint(sv, g, app, &fp);
     if (st) return st;
+    int cls = 0;
+    {
+        std::lock_guard<std::mutex> lk(sv->ctx->mu);
+        Graph *gp = get_graph(sv->ctx, g);
+        if (!gp) return KHZ_ERR_ARG;
+        for (uint64_t m = gp->m + 1; m > 1; m >>= 1) ++cls;
+    }
     const double t = now_s();
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         const khz_ticket id = sv->next_ticket++;
-        sv->pending.push_back(ServeRequest{id, g, (int)app, t, fp});
+        sv->pending.push_back(ServeRequest{id, g, (int)app, t, fp, cls});
         sv->results[id] = ServeResult{};
         if (sv->t_first < 0) sv->t_first = t;
         *ticket = id;
