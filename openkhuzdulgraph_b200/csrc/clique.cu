@@ -403,42 +403,32 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
 }
 
-// Degree buckets of the block tiers, heaviest first within each list:
-//   mid list   = (128, 256] then (64, 128]
-//   large list = (1024, kBlockMax] then (512, 1024] then (256, 512]
-// Bucket 5 = overflow (left to the DFS engine), -1 = warp tier.
-__device__ __forceinline__ int bucket_of(uint32_t d, uint32_t warp_max) {
-    if (d <= warp_max) return -1;
-    if (d <= 128) return 0;
-    if (d <= (uint32_t)kMidMax) return 1;
-    if (d <= 512) return 2;
-    if (d <= 1024) return 3;
-    if (d <= (uint32_t)kBlockMax) return 4;
-    return 5;
-}
+// Block-tier lists in exact descending out-degree order, built without the host: a histogram
+// over degrees, one prefix pass, one write pass (a counting sort).  The mid list holds degrees
+// (warp_max, kMidMax], the large list (kMidMax, kBlockMax]; larger degrees go to the DFS engine.
+// Counter layout (unsigned int): hist[kCntDeg], cursor[kCntDeg], base[kCntDeg], then the two
+// list lengths.
+constexpr int kCntDeg = kBlockMax + 1;
+constexpr int kCntCursor = kCntDeg, kCntBase = 2 * kCntDeg, kCntMidLen = 3 * kCntDeg, kCntLargeLen = 3 * kCntDeg + 1;
+constexpr int kCntWords = 3 * kCntDeg + 2;
 
-// classification counters (unsigned int): [0..5] bucket sizes, [6..11] cursors, [12..17] list
-// positions of each bucket, [18] mid list length, [19] large list length
-constexpr int kCntCursor = 6, kCntBase = 12, kCntMidLen = 18, kCntLargeLen = 19;
-
-// pass 1: bucket sizes, and the level-1 extensions (v0, v1) of every start vertex this engine
-// serves (the reference counts one extension per scattered v1, engine.cc:924)
+// pass 1: degree histogram of block-tier start vertices, and the level-1 extensions (v0, v1) of
+// every start vertex this engine serves (the reference counts one per scattered v1, engine.cc:924)
 __global__ void classify_count_kernel(const BJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
                                       uint32_t warp_max, unsigned int *cnt, uint64_t *rows_out) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: whole warps iterate together
     for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < ((n_total + 31) & ~31ull);
          gv += stride) {
-        int b = -2, j = -1;
+        int j = -1;
         uint32_t d = 0;
         if (gv < n_total) {
             j = job_of(jobs, n_jobs, gv);
             d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
-            b = bucket_of(d, warp_max);
+            if (d > warp_max && d <= (uint32_t)kBlockMax) atomicAdd(&cnt[d], 1u);
         }
-        if (b >= 0 && b < 5) atomicAdd(&cnt[b], 1u);
         // one atomic per distinct job per warp
         const unsigned peers = __match_any_sync(kFull, j);
-        const uint64_t mine = (j >= 0 && b != 5) ? d : 0;
+        const uint64_t mine = (j >= 0 && d <= (uint32_t)kBlockMax) ? d : 0;
         uint64_t sum = 0;
         for (int l = 0; l < 32; ++l) {
             const uint64_t v = __shfl_sync(kFull, mine, l);
@@ -449,18 +439,23 @@ __global__ void classify_count_kernel(const BJob *__restrict__ jobs, int n_jobs,
     }
 }
 
-__global__ void classify_prefix_kernel(unsigned int *cnt) {
+__global__ void classify_prefix_kernel(unsigned int *cnt, uint32_t warp_max) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    cnt[kCntBase + 1] = 0;  // mid list: bucket 1 then 0
-    cnt[kCntBase + 0] = cnt[1];
-    cnt[kCntMidLen] = cnt[0] + cnt[1];
-    cnt[kCntBase + 4] = 0;  // large list: 4, 3, 2
-    cnt[kCntBase + 3] = cnt[4];
-    cnt[kCntBase + 2] = cnt[4] + cnt[3];
-    cnt[kCntLargeLen] = cnt[2] + cnt[3] + cnt[4];
+    unsigned int acc = 0;
+    for (int d = kMidMax; d > (int)warp_max; --d) {
+        cnt[kCntBase + d] = acc;
+        acc += cnt[d];
+    }
+    cnt[kCntMidLen] = acc;
+    acc = 0;
+    for (int d = kBlockMax; d > kMidMax; --d) {
+        cnt[kCntBase + d] = acc;
+        acc += cnt[d];
+    }
+    cnt[kCntLargeLen] = acc;
 }
 
-// pass 2: write each block-tier start vertex into its list
+// pass 2: write each block-tier start vertex at its place in its list
 __global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
                                       uint32_t warp_max, unsigned int *cnt, uint32_t *mid_list,
                                       uint32_t *large_list) {
@@ -468,10 +463,9 @@ __global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs,
          gv += (uint64_t)gridDim.x * blockDim.x) {
         const int j = job_of(jobs, n_jobs, gv);
         const uint32_t d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
-        const int b = bucket_of(d, warp_max);
-        if (b < 0 || b >= 5) continue;
-        const unsigned int pos = cnt[kCntBase + b] + atomicAdd(&cnt[kCntCursor + b], 1u);
-        if (b <= 1) mid_list[pos] = (uint32_t)gv;
+        if (d <= warp_max || d > (uint32_t)kBlockMax) continue;
+        const unsigned int pos = cnt[kCntBase + d] + atomicAdd(&cnt[kCntCursor + d], 1u);
+        if (d <= (uint32_t)kMidMax) mid_list[pos] = (uint32_t)gv;
         else large_list[pos] = (uint32_t)gv;
     }
 }
@@ -483,7 +477,7 @@ uint32_t bitmap_block_max_degree() { return kBlockMax; }
 size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap) {
     return Arena::round(sizeof(BJob) * (size_t)std::max(n_jobs, 1)) +
            2 * Arena::round(sizeof(uint32_t) * std::max<uint64_t>(list_cap, 1)) +
-           Arena::round(sizeof(unsigned int) * 32) + Arena::round(sizeof(unsigned long long) * 4);
+           Arena::round(sizeof(unsigned int) * kCntWords) + Arena::round(sizeof(unsigned long long) * 4);
 }
 
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
@@ -500,7 +494,7 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     BJob *d_jobs = arena->take<BJob>(jobs.size());
     L.mid_list = arena->take<uint32_t>(list_cap);
     L.large_list = arena->take<uint32_t>(list_cap);
-    L.cnt = arena->take<unsigned int>(32);
+    L.cnt = arena->take<unsigned int>(kCntWords);
     L.queues = arena->take<unsigned long long>(4);
     if (!d_jobs || !L.mid_list || !L.large_list || !L.cnt || !L.queues) {
         set_error("bitmap launch arena too small");
@@ -545,12 +539,12 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
             ls->phase_launches[phase] += 1;
         }
     };
-    KHZ_CUDA(cudaMemsetAsync(L.cnt, 0, sizeof(unsigned int) * 32, s));
+    KHZ_CUDA(cudaMemsetAsync(L.cnt, 0, sizeof(unsigned int) * kCntWords, s));
     KHZ_CUDA(cudaMemsetAsync(L.queues, 0, sizeof(unsigned long long) * 4, s));
     const int cgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 255) / 256, (uint64_t)L.sms * 8));
     classify_count_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, d_rows);
     if (L.has_mid) {
-        classify_prefix_kernel<<<1, 32, 0, s>>>(L.cnt);
+        classify_prefix_kernel<<<1, 32, 0, s>>>(L.cnt, L.warp_max);
         classify_write_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, L.mid_list,
                                                     L.large_list);
     }
