@@ -139,8 +139,8 @@ __device__ __forceinline__ void row_extents(const Local &g, int tid, int nthr) {
     }
 }
 
-template <bool STATS>
-__device__ __forceinline__ void process_item(const Local &g, int K, int i, int j, const uint64_t *off, Acc &a) {
+template <int K, bool STATS>
+__device__ __forceinline__ void process_item(const Local &g, int i, int j, const uint64_t *off, Acc &a) {
     const uint32_t *ri = g.rows + (size_t)i * g.W;
     const uint32_t *rj = g.rows + (size_t)j * g.W;
     const int lo = max((int)g.rlo[i], (int)g.rlo[j]);
@@ -175,7 +175,7 @@ __device__ __forceinline__ void process_item(const Local &g, int K, int i, int j
 
 // Count over rows [row_begin, d) with stride row_step for a k-clique job; (i, j) items are dealt
 // to the lanes of the calling warp in batches of 32 (k is warp-uniform: one start vertex at a time).
-template <bool STATS>
+template <bool STATS, int KMAX>
 __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, Acc &a) {
     const unsigned lane = lane_id();
     int pc = 0;  // pending items held by lanes [0, pc)
@@ -201,7 +201,8 @@ __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_b
                 my_j = (ww << 5) + nth_set_bit(bits, q - pc);
             }
             if (pc + c >= 32) {
-                process_item<STATS>(g, K, my_i, my_j, off, a);
+                if (KMAX == 4 || K == 4) process_item<4, STATS>(g, my_i, my_j, off, a);
+                else process_item<5, STATS>(g, my_i, my_j, off, a);
                 const int rem = pc + c - 32;
                 if (q < rem) {
                     my_i = i;
@@ -213,7 +214,10 @@ __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_b
             }
         }
     }
-    if (K > 3 && (int)lane < pc) process_item<STATS>(g, K, my_i, my_j, off, a);
+    if (K > 3 && (int)lane < pc) {
+        if (KMAX == 4 || K == 4) process_item<4, STATS>(g, my_i, my_j, off, a);
+        else process_item<5, STATS>(g, my_i, my_j, off, a);
+    }
 }
 
 // warp reduction of the accumulator and one atomicAdd per counter into the job's row
@@ -251,7 +255,7 @@ __device__ __forceinline__ uint64_t *row_of(uint64_t *rows, const BJob &j) { ret
 // Warp tier: one warp per start vertex with dmin <= d <= 64 over all jobs' vertices, taken in
 // descending global index (per job: descending rank, i.e. heaviest first on the oriented DAG).
 constexpr int kWarpHashLog = 7;  // 128-slot table per warp
-template <bool STATS>
+template <bool STATS, int KMAX>
 __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict__ jobs, int n_jobs,
                                                           uint64_t n_total, uint32_t dmin, uint32_t warp_max,
                                                           unsigned long long *queue, uint64_t *rows_out,
@@ -318,7 +322,7 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict
             __syncwarp();
             row_extents(g, lane, 32);
             __syncwarp();
-            count_rows<STATS>(g, jobs[j].k, off, 0, 1, a);
+            count_rows<STATS, KMAX>(g, jobs[j].k, off, 0, 1, a);
         }
     }
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
@@ -339,7 +343,7 @@ __host__ __device__ __forceinline__ size_t block_smem(int dcap) {
 
 // Block tier: one block per start vertex; the list holds global start-vertex indices, heaviest
 // degree bucket first, and its length is read from device memory.
-template <bool STATS>
+template <bool STATS, int KMAX>
 __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ list,
                                     const unsigned int *__restrict__ list_len, int dcap, unsigned long long *queue,
                                     uint64_t *rows_out, uint64_t *phase_bytes) {
@@ -397,7 +401,7 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
         __syncthreads();
         row_extents(g, threadIdx.x, blockDim.x);
         __syncthreads();
-        count_rows<STATS>(g, jobs[j].k, off, wib, warps, a);
+        count_rows<STATS, KMAX>(g, jobs[j].k, off, wib, warps, a);
         __syncthreads();
     }
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
@@ -484,6 +488,8 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
                           int warp_max, Arena *arena, BitmapLaunch *bl, cudaStream_t s) {
     BitmapLaunch L;
     L.warp_max = warp_max == 32 ? 32u : (uint32_t)kWarpMax;
+    L.kmax = 4;
+    for (const auto &j : jobs) L.kmax = std::max(L.kmax, (int)j.k);
     L.n_jobs = (int)jobs.size();
     L.n_total = jobs.empty() ? 0 : jobs.back().vbase + jobs.back().n;
     L.stats = stats;
@@ -513,7 +519,8 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     const int threads[2] = {256, 1024};
     for (int t = 0; t < 2; ++t) {
         const size_t smem = block_smem(dcaps[t]);
-        auto kern = stats ? clique_block_kernel<true> : clique_block_kernel<false>;
+        auto kern = stats ? (L.kmax == 5 ? clique_block_kernel<true, 5> : clique_block_kernel<true, 4>)
+                          : (L.kmax == 5 ? clique_block_kernel<false, 5> : clique_block_kernel<false, 4>);
         // the attribute is per kernel, shared by every prepared launch: always allow the largest
         // footprint so launches prepared earlier with more shared memory stay valid
         KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem(kBlockMax)));
@@ -551,12 +558,12 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
     KHZ_CUDA(cudaGetLastError());
     if (ls) ls->launches += L.has_mid ? 3 : 1;
     mark(0, true);
-    if (L.stats)
-        clique_warp_kernel<true><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 1u, L.warp_max,
-                                                           &L.queues[0], d_rows, pb(0));
-    else
-        clique_warp_kernel<false><<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, 2u, L.warp_max,
-                                                            &L.queues[0], d_rows, pb(0));
+    {
+        auto wk = L.stats ? (L.kmax == 5 ? clique_warp_kernel<true, 5> : clique_warp_kernel<true, 4>)
+                          : (L.kmax == 5 ? clique_warp_kernel<false, 5> : clique_warp_kernel<false, 4>);
+        wk<<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.stats ? 1u : 2u, L.warp_max, &L.queues[0], d_rows,
+                                     pb(0));
+    }
     KHZ_CUDA(cudaGetLastError());
     mark(0, false);
     if (ls) ls->launches += 1;
@@ -566,12 +573,10 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
         const uint32_t *list = t == 0 ? L.mid_list : L.large_list;
         const unsigned int *len = L.cnt + (t == 0 ? kCntMidLen : kCntLargeLen);
         mark(1 + t, true);
-        if (L.stats)
-            clique_block_kernel<true><<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(
-                L.d_jobs, L.n_jobs, list, len, L.block_dcap[t], &L.queues[1 + t], d_rows, pb(1 + t));
-        else
-            clique_block_kernel<false><<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(
-                L.d_jobs, L.n_jobs, list, len, L.block_dcap[t], &L.queues[1 + t], d_rows, pb(1 + t));
+        auto bk = L.stats ? (L.kmax == 5 ? clique_block_kernel<true, 5> : clique_block_kernel<true, 4>)
+                          : (L.kmax == 5 ? clique_block_kernel<false, 5> : clique_block_kernel<false, 4>);
+        bk<<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(L.d_jobs, L.n_jobs, list, len, L.block_dcap[t],
+                                                                       &L.queues[1 + t], d_rows, pb(1 + t));
         KHZ_CUDA(cudaGetLastError());
         mark(1 + t, false);
         if (ls) ls->launches += 1;

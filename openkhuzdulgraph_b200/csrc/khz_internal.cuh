@@ -136,6 +136,7 @@ struct BitmapLaunch {
     unsigned long long *queues = nullptr;
     int large_dcap = 0;
     uint32_t warp_max = 64;  // out-degrees served by one warp (32 or 64)
+    int kmax = 4;            // largest clique size among the jobs (4 or 5: selects the kernel build)
     bool has_mid = false, has_large = false, stats = false;
     int sms = 0;
     size_t block_smem[2] = {0, 0};
