@@ -163,14 +163,16 @@ struct BatchPlan {
     bool own_pinned = false;      // h_final was allocated by the plan
     uint64_t slot_words = 0;      // DFS slot words needed when they are shared
     size_t mem_bytes = 0;
-    cudaStream_t pool_stream = nullptr;  // mem came from the context pool, freed on this stream
+    bool pool_mem = false;               // mem came from the context pool ...
+    cudaStream_t pool_stream = nullptr;  // ... and is released on this stream (null: legacy stream)
+    std::vector<khz_graph> graphs;       // graphs (and oriented views) whose pointers the plan holds
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~BatchPlan() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (mem) {
-            if (pool_stream) cudaFreeAsync(mem, pool_stream);
+            if (pool_mem) cudaFreeAsync(mem, pool_stream);
             else cudaFree(mem);
         }
         if (h_final && own_pinned) cudaFreeHost(h_final);
@@ -321,6 +323,7 @@ int pick_engine(const khz_config &cfg, const AppDef &def, int app, const Graph &
 constexpr unsigned kPlanOwnSlots = 1u;   // the plan owns its DFS slots (else the context's shared ones)
 constexpr unsigned kPlanPinned = 2u;     // the plan owns a pinned result buffer
 constexpr unsigned kPlanPoolMem = 4u;    // device scratch from the context's stream-ordered pool on `s`
+constexpr unsigned kPlanFreeLegacy = 8u; // with kPlanPoolMem: release on the legacy stream (callers sync first)
 
 khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, unsigned opts,
                       std::unique_ptr<BatchPlan> *out) {
@@ -367,6 +370,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     for (int i = 0; i < n; ++i) {
         const AppDef &def = app_def(jobs[i].app);
         P->apps.push_back(jobs[i].app);
+        P->graphs.push_back(jobs[i].graph);  // an oriented view is owned by (and freed with) its source
         for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
         const int engine = pick_engine(ctx->cfg, def, jobs[i].app, *get_graph(ctx, jobs[i].graph));
         if (engine == KHZ_ENGINE_BITMAP && !def.clique) {
@@ -432,7 +436,10 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     cudaError_t e;
     if (opts & kPlanPoolMem) {
         e = cudaMallocFromPoolAsync(&P->mem, bytes, ctx->pool, s);
-        if (e == cudaSuccess) P->pool_stream = s;
+        if (e == cudaSuccess) {
+            P->pool_mem = true;
+            P->pool_stream = (opts & kPlanFreeLegacy) ? nullptr : s;
+        }
     } else {
         e = cudaMalloc(&P->mem, bytes);
     }
@@ -568,7 +575,7 @@ khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, Batch
     }
     khz_job j{g, (int32_t)app, 0};
     std::unique_ptr<BatchPlan> P;
-    khz_status st = build_plan(ctx, &j, 1, s, 0, &P);
+    khz_status st = build_plan(ctx, &j, 1, s, kPlanPoolMem | kPlanFreeLegacy, &P);
     if (st) return st;
     *out = P.get();
     ctx->plans[key] = std::move(P);
@@ -827,8 +834,8 @@ khz_status khz_ctx_destroy(khz_ctx *ctx) {
         for (size_t i = 0; i < ctx->graphs.size(); ++i)
             if (ctx->live[i]) free_graph_memory(&ctx->graphs[i]);
     }
-    cudaDeviceSynchronize();
     ctx->plans.clear();
+    cudaDeviceSynchronize();  // the plans' pooled scratch is released on the legacy stream
     if (ctx->shared_slots) cudaFree(ctx->shared_slots);
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
@@ -853,7 +860,8 @@ khz_status khz_ctx_set_config(khz_ctx *ctx, const khz_config *cfg) {
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->cfg = *cfg;
-    ctx->plans.clear();  // prepared launches of the previous configuration
+    cudaDeviceSynchronize();  // a prepared launch of the previous configuration may still run
+    ctx->plans.clear();
     if (ctx->cfg.dfs_warps_per_sm <= 0) ctx->cfg.dfs_warps_per_sm = 16;
     if (ctx->cfg.dfs_chunk <= 0) ctx->cfg.dfs_chunk = 8;
     return KHZ_OK;
@@ -1085,9 +1093,17 @@ khz_status khz_graph_free(khz_ctx *ctx, khz_graph h) {
     if (!g) return KHZ_ERR_ARG;
     // work on any stream may still read the graph: order the release after all of it
     KHZ_CUDA(cudaDeviceSynchronize());
-    ctx->plans.clear();  // prepared launches hold the graph's device pointers
-    AllocScope scope(ctx->pool, nullptr);
     const khz_graph ov = g->oriented_view;
+    // prepared launches that hold the graph's (or its oriented view's) device pointers go with it;
+    // the others stay cached
+    for (auto it = ctx->plans.begin(); it != ctx->plans.end();) {
+        const auto &gs = it->second->graphs;
+        if (std::find(gs.begin(), gs.end(), h) != gs.end())
+            it = ctx->plans.erase(it);
+        else
+            ++it;
+    }
+    AllocScope scope(ctx->pool, nullptr);
     free_graph_memory(g);
     ctx->live[h - 1] = false;
     if (ov) {
@@ -1495,6 +1511,7 @@ khz_status khz_autotune(khz_ctx *ctx, const khz_job *jobs, int n_jobs, int reps,
     cudaStreamDestroy(s);
     ctx->cfg = st == KHZ_OK ? best : base;
     ctx->cfg.want_algo_bytes = base.want_algo_bytes;
+    cudaDeviceSynchronize();
     ctx->plans.clear();
     if (st) return st;
     if (report) {
