@@ -31,7 +31,7 @@ namespace {
 
 constexpr int kWarpMax = 64;          // warp tier: d <= 64 -> 2 words per row
 constexpr int kMidMax = 256;          // mid block tier
-constexpr int kBlockMax = 1216;       // large block tier: 1216 rows x 38 words = 180 KiB (+ hash 24 KiB)
+constexpr int kBlockMax = 1216;       // large block tier: 1216 rows x 39 words = 185 KiB (+ hash 24 KiB)
 
 // position of the n-th (0-based) set bit of x; x must have more than n set bits
 __device__ __forceinline__ int nth_set_bit(uint32_t x, int n) {
@@ -64,7 +64,9 @@ constexpr uint32_t kEmpty = 0xffffffffu;
 // The subgraph induced on C = N+(v0), in shared memory:
 //   c[d]            the candidates (sorted vertex ids)
 //   hkey/hidx[T]    open-addressing hash of c: vertex id -> position (T = 2^logt >= 2d)
-//   rows[d * W]     bit j of row i set iff c[j] in N+(c[i])   (only j > i)
+//   rows[d * S]     bit j of row i set iff c[j] in N+(c[i])   (only j > i); W = ceil(d / 32)
+//                   words per row at an odd stride S = W | 1, so that lanes reading the same
+//                   word offset of different rows hit different shared-memory banks
 //   rlo/rhi[d]      first / one-past-last non-zero word of each row
 struct Local {
     uint32_t *c;
@@ -72,7 +74,7 @@ struct Local {
     uint16_t *hidx;
     uint32_t *rows;
     uint16_t *rlo, *rhi;
-    int d, W, logt;
+    int d, W, S, logt;
     __device__ __forceinline__ uint32_t slot(uint32_t x) const { return (x * 0x9E3779B1u) >> (32 - logt); }
     __device__ __forceinline__ int find(uint32_t x) const {
         const uint32_t mask = (1u << logt) - 1u;
@@ -98,27 +100,56 @@ __device__ __forceinline__ void hash_insert(const Local &g, int tid, int nthr) {
 }
 
 // Build rows [row_begin, d - 1) with stride row_step; the calling warp owns those rows.
-// Members of N+(c[i]) outside [c[i+1], c[d-1]] cannot be in C and are skipped.
+// Only members of N+(c[i]) in [c[i+1], c[d-1]] can be in C.  32 evenly spaced splitters of the
+// list, read in one load, bound that range to within one splitter gap at each end, so a row costs
+// one round trip plus one per 64 scanned entries (lists of <= 32 entries are the splitters
+// themselves).  The list offsets of the warp's next 32 rows are fetched together, one per lane.
 __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
                            int row_begin, int row_step) {
     const unsigned lane = lane_id();
     const int d = g.d;
     const uint32_t hi_val = g.c[d - 1];
-    for (int i = row_begin; i < d - 1; i += row_step) {
-        const uint32_t v = g.c[i];
-        const uint64_t b0 = __ldg(off + v);
-        const uint32_t len = (uint32_t)(__ldg(off + v + 1) - b0);
-        const uint32_t *L = adj + b0;
-        const uint32_t start = lower_bound_u32(L, 0, len, g.c[i + 1]);
-        uint32_t *row = g.rows + (size_t)i * g.W;
-        for (uint32_t b = start; b < len; b += 32) {
-            const uint32_t idx = b + lane;
-            const uint32_t x = idx < len ? __ldg(L + idx) : kEmpty;
-            if (x <= hi_val) {
-                const int j = g.find(x);
-                if (j >= 0) atomicOr(row + (j >> 5), 1u << (j & 31));
+    for (int i0 = row_begin; i0 < d - 1; i0 += 32 * row_step) {
+        const int mine = i0 + (int)lane * row_step;
+        uint64_t my_b = 0;
+        uint32_t my_len = 0;
+        if (mine < d - 1) {
+            const uint32_t v = g.c[mine];
+            my_b = __ldg(off + v);
+            my_len = (uint32_t)(__ldg(off + v + 1) - my_b);
+        }
+        const int nrows = min(32, (d - 1 - i0 + row_step - 1) / row_step);
+        for (int r = 0; r < nrows; ++r) {
+            const int i = i0 + r * row_step;
+            const uint64_t b0 = __shfl_sync(kFull, my_b, r);
+            const uint32_t len = __shfl_sync(kFull, my_len, r);
+            const uint32_t *L = adj + b0;
+            const uint32_t lo_val = g.c[i + 1];
+            uint32_t *row = g.rows + (size_t)i * g.S;
+            auto probe = [&](uint32_t x) {
+                if (x >= lo_val && x <= hi_val) {
+                    const int j = g.find(x);
+                    if (j >= 0) atomicOr(row + (j >> 5), 1u << (j & 31));
+                }
+            };
+            const uint64_t step = ((uint64_t)len + 31) >> 5;
+            const uint64_t sidx = lane * step;
+            const uint32_t sp = sidx < len ? __ldg(L + sidx) : kEmpty;
+            if (step <= 1) {
+                probe(sp);
+                continue;
             }
-            if (__shfl_sync(kFull, x, 31) >= hi_val) break;
+            const uint64_t k_lo = __popc(__ballot_sync(kFull, sp < lo_val));
+            const uint64_t k_hi = __popc(__ballot_sync(kFull, sp <= hi_val));
+            const uint64_t begin = k_lo == 0 ? 0 : (k_lo - 1) * step + 1;
+            const uint64_t end = min((uint64_t)len, k_hi * step);
+            for (uint64_t b = begin; b < end; b += 64) {
+                const uint64_t i0x = b + lane, i1x = b + 32 + lane;
+                const uint32_t x0 = i0x < end ? __ldg(L + i0x) : kEmpty;
+                const uint32_t x1 = i1x < end ? __ldg(L + i1x) : kEmpty;
+                probe(x0);
+                probe(x1);
+            }
         }
     }
 }
@@ -126,7 +157,7 @@ __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, con
 // first / one-past-last non-zero word of rows [tid, d) step nthr
 __device__ __forceinline__ void row_extents(const Local &g, int tid, int nthr) {
     for (int i = tid; i < g.d; i += nthr) {
-        const uint32_t *r = g.rows + (size_t)i * g.W;
+        const uint32_t *r = g.rows + (size_t)i * g.S;
         int lo = g.W, hi = 0;
         for (int w = (i + 1) >> 5; w < g.W; ++w) {
             if (r[w]) {
@@ -141,8 +172,8 @@ __device__ __forceinline__ void row_extents(const Local &g, int tid, int nthr) {
 
 template <int K, bool STATS>
 __device__ __forceinline__ void process_item(const Local &g, int i, int j, const uint64_t *off, Acc &a) {
-    const uint32_t *ri = g.rows + (size_t)i * g.W;
-    const uint32_t *rj = g.rows + (size_t)j * g.W;
+    const uint32_t *ri = g.rows + (size_t)i * g.S;
+    const uint32_t *rj = g.rows + (size_t)j * g.S;
     const int lo = max((int)g.rlo[i], (int)g.rlo[j]);
     const int hi = min((int)g.rhi[i], (int)g.rhi[j]);
     uint32_t s = 0;
@@ -162,7 +193,7 @@ __device__ __forceinline__ void process_item(const Local &g, int i, int j, const
         while (m) {
             const int l = (w1 << 5) + __ffs(m) - 1;
             m &= m - 1;
-            const uint32_t *rl = g.rows + (size_t)l * g.W;
+            const uint32_t *rl = g.rows + (size_t)l * g.S;
             const int lo3 = max(lo, (int)g.rlo[l]);
             const int hi3 = min(hi, (int)g.rhi[l]);
             uint32_t t = 0;
@@ -173,51 +204,98 @@ __device__ __forceinline__ void process_item(const Local &g, int i, int j, const
     }
 }
 
-// Count over rows [row_begin, d) with stride row_step for a k-clique job; (i, j) items are dealt
-// to the lanes of the calling warp in batches of 32 (k is warp-uniform: one start vertex at a time).
+// Items (i, j) = the set bits j of row i, dealt to the lanes of the calling warp in batches of
+// 32.  Each lane holds one unit (row u_row, word u_word, its bits); an inclusive scan of the
+// units' popcounts numbers their items, and each free lane finds its item's unit by a 5-step
+// search over the lanes' prefix sums.  A partial batch (lanes [0, pc) hold items) carries over to
+// the next call.  k is warp-uniform (one start vertex at a time).
 template <bool STATS, int KMAX>
-__device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, Acc &a) {
-    const unsigned lane = lane_id();
-    int pc = 0;  // pending items held by lanes [0, pc)
-    int my_i = 0, my_j = 0;
-    for (int i = row_begin; i < g.d; i += row_step) {
-        const uint32_t *ri = g.rows + (size_t)i * g.W;
-        const int lo = g.rlo[i], hi = g.rhi[i];
-        uint32_t pop = 0;
-        for (int w = lo; w < hi; ++w) pop += __popc(ri[w]);
-        if (lane == 0) a.t3 += pop;
-        if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]) + pop);
-        if (K == 3) {
-            if (lane == 0) a.cnt += pop;
-            continue;
+__device__ __forceinline__ void deal_units(const Local &g, int K, const uint64_t *off, int u_row, int u_word,
+                                           uint32_t bits, int &pc, int &my_i, int &my_j, Acc &a) {
+    const int lane = (int)lane_id();
+    const int c = __popc(bits);
+    a.t3 += c;
+    if (STATS) a.bytes += 4ull * c;
+    if (K == 3) {
+        a.cnt += c;
+        return;
+    }
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(kFull, incl, 31);
+    const int excl = incl - c;
+    for (int consumed = 0; consumed < total;) {
+        const int avail = min(32 - pc, total - consumed);
+        const int t = consumed + lane - pc;
+        int w = 0;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const int e = __shfl_sync(kFull, excl, w + s);
+            if (e <= t) w += s;
         }
-        for (int ww = lo; ww < hi; ++ww) {
-            const uint32_t bits = ri[ww];
-            const int c = __popc(bits);
-            if (c == 0) continue;
-            const int q = (int)lane;
-            if (q >= pc && q < pc + c) {
-                my_i = i;
-                my_j = (ww << 5) + nth_set_bit(bits, q - pc);
-            }
-            if (pc + c >= 32) {
-                if (KMAX == 4 || K == 4) process_item<4, STATS>(g, my_i, my_j, off, a);
-                else process_item<5, STATS>(g, my_i, my_j, off, a);
-                const int rem = pc + c - 32;
-                if (q < rem) {
-                    my_i = i;
-                    my_j = (ww << 5) + nth_set_bit(bits, (32 - pc) + q);
-                }
-                pc = rem;
-            } else {
-                pc += c;
-            }
+        const uint32_t wb = __shfl_sync(kFull, bits, w);
+        const int we = __shfl_sync(kFull, excl, w);
+        const int wr = __shfl_sync(kFull, u_row, w);
+        const int ww = __shfl_sync(kFull, u_word, w);
+        if (lane >= pc && lane < pc + avail) {
+            my_i = wr;
+            my_j = (ww << 5) + nth_set_bit(wb, t - we);
+        }
+        consumed += avail;
+        pc += avail;
+        if (pc == 32) {
+            if (KMAX == 4 || K == 4) process_item<4, STATS>(g, my_i, my_j, off, a);
+            else process_item<5, STATS>(g, my_i, my_j, off, a);
+            pc = 0;
         }
     }
-    if (K > 3 && (int)lane < pc) {
+}
+
+template <bool STATS, int KMAX>
+__device__ __forceinline__ void deal_flush(const Local &g, int K, const uint64_t *off, int pc, int my_i, int my_j,
+                                           Acc &a) {
+    if (K > 3 && (int)lane_id() < pc) {
         if (KMAX == 4 || K == 4) process_item<4, STATS>(g, my_i, my_j, off, a);
         else process_item<5, STATS>(g, my_i, my_j, off, a);
     }
+}
+
+// Count over rows [row_begin, d) with stride row_step for a k-clique job: one unit per word of
+// the row's non-zero extent, 32 words at a time.
+template <bool STATS, int KMAX>
+__device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, Acc &a) {
+    const int lane = (int)lane_id();
+    int pc = 0, my_i = 0, my_j = 0;
+    for (int i = row_begin; i < g.d; i += row_step) {
+        const uint32_t *ri = g.rows + (size_t)i * g.S;
+        const int lo = g.rlo[i], hi = g.rhi[i];
+        if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]));
+        for (int base = lo; base < hi; base += 32) {
+            const int w = base + lane;
+            deal_units<STATS, KMAX>(g, K, off, i, w, w < hi ? ri[w] : 0u, pc, my_i, my_j, a);
+        }
+    }
+    deal_flush<STATS, KMAX>(g, K, off, pc, my_i, my_j, a);
+}
+
+// The same over all rows of a warp-tier start vertex (W = 2 words per row): 16 rows per round.
+template <bool STATS, int KMAX>
+__device__ void count_rows_small(const Local &g, int K, const uint64_t *off, Acc &a) {
+    const int lane = (int)lane_id();
+    int pc = 0, my_i = 0, my_j = 0;
+    if (STATS)
+        for (int i = lane; i < g.d; i += 32) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]));
+    for (int u0 = 0; u0 < 2 * g.d; u0 += 32) {
+        const int u = u0 + lane;
+        const int i = u >> 1, w = u & 1;
+        const uint32_t bits = i < g.d ? g.rows[(size_t)i * g.S + w] : 0u;
+        deal_units<STATS, KMAX>(g, K, off, i, w, bits, pc, my_i, my_j, a);
+    }
+    deal_flush<STATS, KMAX>(g, K, off, pc, my_i, my_j, a);
 }
 
 // warp reduction of the accumulator and one atomicAdd per counter into the job's row
@@ -261,9 +339,10 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict
                                                           unsigned long long *queue, uint64_t *rows_out,
                                                           uint64_t *phase_bytes) {
     constexpr int W = kWarpMax / 32;
+    constexpr int S = W | 1;
     constexpr int T = 1 << kWarpHashLog;
     __shared__ uint32_t s_c[8][kWarpMax];
-    __shared__ uint32_t s_rows[8][kWarpMax * W];
+    __shared__ uint32_t s_rows[8][kWarpMax * S];
     __shared__ uint32_t s_hkey[8][T];
     __shared__ uint16_t s_hidx[8][T];
     __shared__ uint16_t s_rlo[8][kWarpMax], s_rhi[8][kWarpMax];
@@ -277,6 +356,7 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict
     g.rlo = s_rlo[wib];
     g.rhi = s_rhi[wib];
     g.W = W;
+    g.S = S;
     g.logt = kWarpHashLog;
     Acc a = {0, 0, 0, 0};
     int cur_job = -1;
@@ -313,7 +393,7 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict
             const uint64_t b0 = __ldg(off + v0);
             __syncwarp();
             for (int t = lane; t < kWarpMax; t += 32) g.c[t] = t < g.d ? __ldg(adj + b0 + t) : kEmpty;
-            for (int t = lane; t < kWarpMax * W; t += 32) g.rows[t] = 0;
+            for (int t = lane; t < kWarpMax * S; t += 32) g.rows[t] = 0;
             for (int t = lane; t < T; t += 32) g.hkey[t] = kEmpty;
             __syncwarp();
             hash_insert(g, lane, 32);
@@ -322,7 +402,7 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict
             __syncwarp();
             row_extents(g, lane, 32);
             __syncwarp();
-            count_rows<STATS, KMAX>(g, jobs[j].k, off, 0, 1, a);
+            count_rows_small<STATS, KMAX>(g, jobs[j].k, off, a);
         }
     }
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
@@ -337,7 +417,7 @@ __host__ __device__ __forceinline__ int block_logt(int dcap) {
 __host__ __device__ __forceinline__ size_t block_smem(int dcap) {
     const size_t dp = (size_t)((dcap + 31) & ~31);
     const size_t t = (size_t)1 << block_logt(dcap);
-    const size_t w = (size_t)((dcap + 31) / 32);
+    const size_t w = (size_t)((dcap + 31) / 32) | 1;
     return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + dp * w * 4;
 }
 
@@ -390,9 +470,10 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
         const uint32_t *adj = jobs[j].adj;
         g.d = (int)odeg(off, v0);
         g.W = (g.d + 31) >> 5;
+        g.S = g.W | 1;
         const uint64_t b0 = __ldg(off + v0);
         for (int t = threadIdx.x; t < g.d; t += blockDim.x) g.c[t] = __ldg(adj + b0 + t);
-        for (int t = threadIdx.x; t < g.d * g.W; t += blockDim.x) g.rows[t] = 0;
+        for (int t = threadIdx.x; t < g.d * g.S; t += blockDim.x) g.rows[t] = 0;
         for (int t = threadIdx.x; t < T; t += blockDim.x) g.hkey[t] = kEmpty;
         __syncthreads();
         hash_insert(g, threadIdx.x, blockDim.x);
