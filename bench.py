@@ -33,6 +33,7 @@ sys.path.insert(0, ROOT)
 SCALE, EDGE_FACTOR, SEED = 22, 16, 1   # defaults; --scale / --edge-factor select a smaller case for profiling
 RMAT_ABC = (0.57, 0.19, 0.19)
 APP = "kautomine_four_clique"
+KNOWN_COUNTS = {(22, 16): 123601255038, (21, 16): 46044614288}
 SAMPLE_MOD = 32      # CPU sample: start vertices with v0 % 32 == 0 (one label class of 32)
 METRIC = "embeddings/s (4-clique, exact uint64 count)"
 WORKLOAD = "4-clique count, R-MAT scale 22 ef 16 (a,b,c)=(0.57,0.19,0.19) seed 1, degree-oriented DAG"
@@ -186,6 +187,10 @@ def ours(args, rank, world, local):
     ref_counts, st_stats = ctx.count(g, APP)
     ctx.set_config(want_algo_bytes=0)
     embeddings = st_stats.num_extensions + ref_counts[0]
+    # 4-clique counts of these generated graphs, equal on the DFS engine (the schedule as written),
+    # the bitmap engine and the symmetric input
+    known = KNOWN_COUNTS.get((args.scale, args.edge_factor))
+    assert known is None or ref_counts[0] == known, (ref_counts, known)
 
     stream = torch.cuda.Stream(dev)
     sptr = stream.cuda_stream

@@ -101,9 +101,12 @@ __device__ __forceinline__ void hash_insert(const Local &g, int tid, int nthr) {
 
 // Build rows [row_begin, d - 1) with stride row_step; the calling warp owns those rows.
 // Only members of N+(c[i]) in [c[i+1], c[d-1]] can be in C.  32 evenly spaced splitters of the
-// list, read in one load, bound that range to within one splitter gap at each end, so a row costs
-// one round trip plus one per 64 scanned entries (lists of <= 32 entries are the splitters
-// themselves).  The list offsets of the warp's next 32 rows are fetched together, one per lane.
+// list, read in one load, bound that range to within one splitter gap at each end (lists of <= 32
+// entries are the splitters themselves); the range is then read kScanUnroll x 32 entries per
+// round with all loads of a round in flight together.  The list offsets of the warp's next 32 rows
+// are fetched together, one per lane, and the next row's splitters are loaded before the current
+// row is scanned, so a row's round trips overlap the previous row's work.
+constexpr int kScanUnroll = 4;
 __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
                            int row_begin, int row_step) {
     const unsigned lane = lane_id();
@@ -119,10 +122,20 @@ __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, con
             my_len = (uint32_t)(__ldg(off + v + 1) - my_b);
         }
         const int nrows = min(32, (d - 1 - i0 + row_step - 1) / row_step);
-        for (int r = 0; r < nrows; ++r) {
-            const int i = i0 + r * row_step;
+        // splitter `lane` of row r: entry lane * ceil(len / 32), or kEmpty past the end
+        auto splitter = [&](int r) -> uint32_t {
             const uint64_t b0 = __shfl_sync(kFull, my_b, r);
             const uint32_t len = __shfl_sync(kFull, my_len, r);
+            const uint64_t sidx = lane * (((uint64_t)len + 31) >> 5);
+            return sidx < len ? __ldg(adj + b0 + sidx) : kEmpty;
+        };
+        uint32_t sp_next = splitter(0);
+        for (int r = 0; r < nrows; ++r) {
+            const int i = i0 + r * row_step;
+            const uint32_t sp = sp_next;
+            const uint64_t b0 = __shfl_sync(kFull, my_b, r);
+            const uint32_t len = __shfl_sync(kFull, my_len, r);
+            if (r + 1 < nrows) sp_next = splitter(r + 1);
             const uint32_t *L = adj + b0;
             const uint32_t lo_val = g.c[i + 1];
             uint32_t *row = g.rows + (size_t)i * g.S;
@@ -133,8 +146,6 @@ __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, con
                 }
             };
             const uint64_t step = ((uint64_t)len + 31) >> 5;
-            const uint64_t sidx = lane * step;
-            const uint32_t sp = sidx < len ? __ldg(L + sidx) : kEmpty;
             if (step <= 1) {
                 probe(sp);
                 continue;
@@ -143,12 +154,15 @@ __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, con
             const uint64_t k_hi = __popc(__ballot_sync(kFull, sp <= hi_val));
             const uint64_t begin = k_lo == 0 ? 0 : (k_lo - 1) * step + 1;
             const uint64_t end = min((uint64_t)len, k_hi * step);
-            for (uint64_t b = begin; b < end; b += 64) {
-                const uint64_t i0x = b + lane, i1x = b + 32 + lane;
-                const uint32_t x0 = i0x < end ? __ldg(L + i0x) : kEmpty;
-                const uint32_t x1 = i1x < end ? __ldg(L + i1x) : kEmpty;
-                probe(x0);
-                probe(x1);
+            for (uint64_t b = begin; b < end; b += 32 * kScanUnroll) {
+                uint32_t x[kScanUnroll];
+#pragma unroll
+                for (int u = 0; u < kScanUnroll; ++u) {
+                    const uint64_t ix = b + 32 * u + lane;
+                    x[u] = ix < end ? __ldg(L + ix) : kEmpty;
+                }
+#pragma unroll
+                for (int u = 0; u < kScanUnroll; ++u) probe(x[u]);
             }
         }
     }
@@ -332,9 +346,9 @@ __device__ __forceinline__ uint64_t *row_of(uint64_t *rows, const BJob &j) { ret
 
 // Warp tier: one warp per start vertex with dmin <= d <= 64 over all jobs' vertices, taken in
 // descending global index (per job: descending rank, i.e. heaviest first on the oriented DAG).
-constexpr int kWarpHashLog = 7;  // 128-slot table per warp
+constexpr int kWarpHashLog = 8;  // 256-slot table per warp (at least 4 slots per candidate)
 template <bool STATS, int KMAX>
-__global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict__ jobs, int n_jobs,
+__global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restrict__ jobs, int n_jobs,
                                                           uint64_t n_total, uint32_t dmin, uint32_t warp_max,
                                                           unsigned long long *queue, uint64_t *rows_out,
                                                           uint64_t *phase_bytes) {
@@ -410,8 +424,11 @@ __global__ void __launch_bounds__(256) clique_warp_kernel(const BJob *__restrict
 
 // shared-memory footprint of a block-tier launch serving out-degrees up to dcap
 __host__ __device__ __forceinline__ int block_logt(int dcap) {
+    // hash slots per candidate: 8 (almost every miss ends at the first slot) where shared memory
+    // allows, 2 for the largest candidate sets
+    const int per = dcap <= kMidMax ? 8 : 2;
     int l = 5;
-    while ((1 << l) < 2 * dcap) ++l;
+    while ((1 << l) < per * dcap) ++l;
     return l;
 }
 __host__ __device__ __forceinline__ size_t block_smem(int dcap) {
