@@ -102,7 +102,10 @@ typedef struct khz_config {
     int32_t dfs_chunk;         /* level-1 candidates claimed per warp per grab (0 = default) */
     int32_t bitmap_warp_max;   /* largest out-degree served by one warp in the bitmap engine (32|64) */
     int32_t bitmap_block_warps;/* warps per block of the bitmap engine's block tier */
-    int32_t reserved[10];
+    int32_t bitmap_hub_rows;   /* bitmap engine: rows of the hub adjacency triangle over the
+                                  highest-ranked vertices (0 = auto, -1 = none, else rounded down
+                                  to a multiple of 32 and capped at the vertex count) */
+    int32_t reserved[9];
 } khz_config;
 
 /* ---- context ---------------------------------------------------------------------- */

@@ -61,6 +61,20 @@ __device__ __forceinline__ uint32_t odeg(const uint64_t *off, uint32_t v) {
 
 constexpr uint32_t kEmpty = 0xffffffffu;
 
+// Hub triangle.  For the H highest-ranked vertices (ids n - H .. n - 1 of the oriented graph,
+// whose out-lists hold only larger ids, so ids of the same range) the adjacency is kept as a bit
+// triangle: row h (vertex n - H + h) holds columns c > h, stored from word (h + 1) / 32 on.
+// A row of the induced subgraph whose vertex is a hub is then read from the triangle with one
+// bit test per candidate instead of a scan of the vertex's out-list.
+constexpr uint32_t kHubRowsAuto = 32768;       // 64 MiB triangle
+constexpr uint64_t kHubMinEdges = 1ull << 22;  // auto: graphs of at least 4 Mi oriented edges
+
+// first word of row h: the sum over rows k < h of (wh - (k + 1) / 32) words
+__host__ __device__ __forceinline__ uint64_t hub_row_offset(uint32_t h, uint32_t wh) {
+    const uint64_t q = h >> 5, r = h & 31;
+    return (uint64_t)h * wh - (16 * q * (q - 1) + q * (r + 1));
+}
+
 // The subgraph induced on C = N+(v0), in shared memory:
 //   c[d]            the candidates (sorted vertex ids)
 //   hkey/hidx[T]    open-addressing hash of c: vertex id -> position (T = 2^logt >= 2d)
@@ -75,6 +89,8 @@ struct Local {
     uint32_t *rows;
     uint16_t *rlo, *rhi;
     int d, W, S, logt;
+    const uint32_t *hub;  // the job's hub triangle, or null
+    uint32_t hub_base, hub_wh;
     __device__ __forceinline__ uint32_t slot(uint32_t x) const { return (x * 0x9E3779B1u) >> (32 - logt); }
     __device__ __forceinline__ int find(uint32_t x) const {
         const uint32_t mask = (1u << logt) - 1u;
@@ -105,8 +121,38 @@ __device__ __forceinline__ void hash_insert(const Local &g, int tid, int nthr) {
 // entries are the splitters themselves); the range is then read kScanUnroll x 32 entries per
 // round with all loads of a round in flight together.  The list offsets of the warp's next 32 rows
 // are fetched together, one per lane, and the next row's splitters are loaded before the current
-// row is scanned, so a row's round trips overlap the previous row's work.
+// row is scanned, so a row's round trips overlap the previous row's work.  Rows of hub vertices
+// come from the job's hub triangle instead.
 constexpr int kScanUnroll = 4;
+
+// Row i of a hub vertex from the triangle: lane l tests candidate j = 32 w + l (j > i), and the
+// ballot over the warp is word w of the row, stored whole (the calling warp owns the row).
+constexpr int kHubUnroll = 2;
+__device__ __forceinline__ void hub_row(const Local &g, int i) {
+    const int lane = (int)lane_id();
+    const uint32_t h = g.c[i] - g.hub_base;
+    const uint32_t *hrow = g.hub + hub_row_offset(h, g.hub_wh);
+    const uint32_t wb = (h + 1) >> 5;
+    uint32_t *row = g.rows + (size_t)i * g.S;
+    for (int w = (i + 1) >> 5; w < g.W; w += kHubUnroll) {
+        bool bit[kHubUnroll];
+#pragma unroll
+        for (int u = 0; u < kHubUnroll; ++u) {
+            const int j = ((w + u) << 5) + lane;
+            bit[u] = false;
+            if (j > i && j < g.d) {
+                const uint32_t cc = g.c[j] - g.hub_base;
+                bit[u] = (__ldg(hrow + ((cc >> 5) - wb)) >> (cc & 31)) & 1u;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kHubUnroll; ++u) {
+            const unsigned m = __ballot_sync(kFull, bit[u]);
+            if (lane == 0 && w + u < g.W) row[w + u] = m;
+        }
+    }
+}
+
 __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
                            int row_begin, int row_step) {
     const unsigned lane = lane_id();
@@ -122,16 +168,22 @@ __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, con
             my_len = (uint32_t)(__ldg(off + v + 1) - my_b);
         }
         const int nrows = min(32, (d - 1 - i0 + row_step - 1) / row_step);
-        // splitter `lane` of row r: entry lane * ceil(len / 32), or kEmpty past the end
+        // splitter `lane` of row r: entry lane * ceil(len / 32), or kEmpty past the end (or for
+        // a hub row, which needs none)
         auto splitter = [&](int r) -> uint32_t {
             const uint64_t b0 = __shfl_sync(kFull, my_b, r);
             const uint32_t len = __shfl_sync(kFull, my_len, r);
+            if (g.hub && g.c[i0 + r * row_step] >= g.hub_base) return kEmpty;
             const uint64_t sidx = lane * (((uint64_t)len + 31) >> 5);
             return sidx < len ? __ldg(adj + b0 + sidx) : kEmpty;
         };
         uint32_t sp_next = splitter(0);
         for (int r = 0; r < nrows; ++r) {
             const int i = i0 + r * row_step;
+            if (g.hub && g.c[i] >= g.hub_base) {
+                hub_row(g, i);
+                continue;
+            }
             const uint32_t sp = sp_next;
             const uint64_t b0 = __shfl_sync(kFull, my_b, r);
             const uint32_t len = __shfl_sync(kFull, my_len, r);
@@ -404,6 +456,9 @@ __global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restr
             }
             const uint64_t *off = jobs[j].off;
             const uint32_t *adj = jobs[j].adj;
+            g.hub = jobs[j].hub;
+            g.hub_base = jobs[j].n - jobs[j].hub_rows;
+            g.hub_wh = jobs[j].hub_rows >> 5;
             const uint64_t b0 = __ldg(off + v0);
             __syncwarp();
             for (int t = lane; t < kWarpMax; t += 32) g.c[t] = t < g.d ? __ldg(adj + b0 + t) : kEmpty;
@@ -485,6 +540,9 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
         }
         const uint64_t *off = jobs[j].off;
         const uint32_t *adj = jobs[j].adj;
+        g.hub = jobs[j].hub;
+        g.hub_base = jobs[j].n - jobs[j].hub_rows;
+        g.hub_wh = jobs[j].hub_rows >> 5;
         g.d = (int)odeg(off, v0);
         g.W = (g.d + 31) >> 5;
         g.S = g.W | 1;
@@ -503,6 +561,24 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
         __syncthreads();
     }
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
+}
+
+// The hub triangle of one job (zeroed beforehand): one warp per hub row.
+__global__ void hub_build_kernel(const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj, uint32_t n,
+                                 uint32_t rows, uint32_t *hub) {
+    const uint32_t base = n - rows, wh = rows >> 5;
+    const unsigned lane = lane_id();
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < rows; h += nw) {
+        const uint32_t u = base + h;
+        const uint64_t e = off[u + 1];
+        uint32_t *row = hub + hub_row_offset(h, wh);
+        const uint32_t wb = (h + 1) >> 5;
+        for (uint64_t t = off[u] + lane; t < e; t += 32) {
+            const uint32_t c = adj[t] - base;  // > h: out-lists hold larger ids only
+            atomicOr(row + ((c >> 5) - wb), 1u << (c & 31));
+        }
+    }
 }
 
 // Block-tier lists in exact descending out-degree order, built without the host: a histogram
@@ -576,10 +652,20 @@ __global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs,
 
 uint32_t bitmap_block_max_degree() { return kBlockMax; }
 
-size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap) {
-    return Arena::round(sizeof(BJob) * (size_t)std::max(n_jobs, 1)) +
-           2 * Arena::round(sizeof(uint32_t) * std::max<uint64_t>(list_cap, 1)) +
-           Arena::round(sizeof(unsigned int) * kCntWords) + Arena::round(sizeof(unsigned long long) * 4);
+uint32_t bitmap_hub_rows(int cfg_rows, uint32_t n, uint64_t m) {
+    if (cfg_rows < 0) return 0;
+    const uint32_t want = cfg_rows == 0 ? (m >= kHubMinEdges ? kHubRowsAuto : 0u) : (uint32_t)cfg_rows;
+    return std::min(want, n) & ~31u;
+}
+
+static size_t hub_words(uint32_t rows) { return rows ? (size_t)hub_row_offset(rows, rows >> 5) : 0; }
+
+size_t bitmap_arena_bytes(const std::vector<BJob> &jobs, uint64_t list_cap) {
+    size_t b = Arena::round(sizeof(BJob) * std::max<size_t>(jobs.size(), 1)) +
+               2 * Arena::round(sizeof(uint32_t) * std::max<uint64_t>(list_cap, 1)) +
+               Arena::round(sizeof(unsigned int) * kCntWords) + Arena::round(sizeof(unsigned long long) * 4);
+    for (const auto &j : jobs) b += Arena::round(sizeof(uint32_t) * hub_words(j.hub_rows));
+    return b;
 }
 
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
@@ -604,8 +690,20 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
         set_error("bitmap launch arena too small");
         return KHZ_ERR_OOM;
     }
-    if (!jobs.empty())
-        KHZ_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(BJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+    std::vector<BJob> dj(jobs);
+    for (auto &j : dj) {
+        j.hub = nullptr;
+        if (!j.hub_rows) continue;
+        uint32_t *h = arena->take<uint32_t>(hub_words(j.hub_rows));
+        if (!h) {
+            set_error("bitmap launch arena too small");
+            return KHZ_ERR_OOM;
+        }
+        j.hub = h;
+        L.hubs.push_back(j);
+    }
+    if (!dj.empty())
+        KHZ_CUDA(cudaMemcpyAsync(d_jobs, dj.data(), sizeof(BJob) * dj.size(), cudaMemcpyHostToDevice, s));
     L.d_jobs = d_jobs;
     int dev = 0;
     KHZ_CUDA(cudaGetDevice(&dev));
@@ -646,6 +744,12 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
     };
     KHZ_CUDA(cudaMemsetAsync(L.cnt, 0, sizeof(unsigned int) * kCntWords, s));
     KHZ_CUDA(cudaMemsetAsync(L.queues, 0, sizeof(unsigned long long) * 4, s));
+    for (const auto &j : L.hubs) {
+        KHZ_CUDA(cudaMemsetAsync(const_cast<uint32_t *>(j.hub), 0, sizeof(uint32_t) * hub_words(j.hub_rows), s));
+        hub_build_kernel<<<std::max(1, std::min<int>(L.sms * 8, (int)(j.hub_rows / 8))), 256, 0, s>>>(
+            j.off, j.adj, j.n, j.hub_rows, const_cast<uint32_t *>(j.hub));
+        if (ls) ls->launches += 1;
+    }
     const int cgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 255) / 256, (uint64_t)L.sms * 8));
     classify_count_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, d_rows);
     if (L.has_mid) {

@@ -379,7 +379,8 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             Graph *og = nullptr;
             khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
             if (st) return st;
-            bjobs.push_back(BJob{og->off, og->adj, og->n, 3, vbase, (uint32_t)i, 0});
+            bjobs.push_back(BJob{og->off, og->adj, og->n, 3, vbase, (uint32_t)i,
+                                 bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m), nullptr});
             vbase += og->n;
             bm_entries += og->m;
             bmax = std::max(bmax, og->max_degree);
@@ -395,7 +396,8 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             Graph *og = nullptr;
             khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
             if (st) return st;
-            BJob b{og->off, og->adj, og->n, def.clique_k, vbase, (uint32_t)i, 0};
+            BJob b{og->off, og->adj, og->n, def.clique_k, vbase, (uint32_t)i,
+                   bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m), nullptr};
             bjobs.push_back(b);
             vbase += og->n;
             bm_entries += og->m;
@@ -428,7 +430,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     size_t bytes = 2 * Arena::round(sizeof(uint64_t) * kRowWords * n) + Arena::round(sizeof(uint32_t) * mult.size()) +
                    Arena::round(sizeof(uint64_t) * n) + Arena::round(sizeof(unsigned int)) +
                    Arena::round(sizeof(uint64_t) * kPhases);
-    if (P->has_bitmap) bytes += bitmap_arena_bytes((int)bjobs.size(), list_cap);
+    if (P->has_bitmap) bytes += bitmap_arena_bytes(bjobs, list_cap);
     if (P->has_wedge) bytes += wedge_arena_bytes((int)wjobs.size(), wbase, wedge_workers(wmax_n), wmax_n);
     if (!mjobs.empty()) bytes += Arena::round(sizeof(MJob) * mjobs.size());
     if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
@@ -566,8 +568,8 @@ khz_status fill_stats(khz_ctx *ctx, BatchPlan *P, const LaunchStats &ls, bool ti
 // the cached prepared launch of one (graph, app) under the current configuration
 khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, BatchPlan **out) {
     char key[160];
-    snprintf(key, sizeof(key), "%u/%d/%d/%d/%d/%d/%d", g, app, ctx->cfg.engine, ctx->cfg.want_algo_bytes,
-             ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, ctx->cfg.bitmap_warp_max);
+    snprintf(key, sizeof(key), "%u/%d/%d/%d/%d/%d/%d/%d", g, app, ctx->cfg.engine, ctx->cfg.want_algo_bytes,
+             ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, ctx->cfg.bitmap_warp_max, ctx->cfg.bitmap_hub_rows);
     auto it = ctx->plans.find(key);
     if (it != ctx->plans.end()) {
         *out = it->second.get();

@@ -108,7 +108,8 @@ struct BJob {
     int32_t k;          // clique size 3, 4 or 5
     uint64_t vbase;
     uint32_t out_row;
-    uint32_t pad;
+    uint32_t hub_rows;  // rows H of the hub triangle (vertices n - H .. n - 1), 0 = none
+    const uint32_t *hub;  // the triangle (set by bitmap_prepare)
 };
 
 // bump allocator over one device allocation
@@ -141,6 +142,7 @@ struct BitmapLaunch {
     int sms = 0;
     size_t block_smem[2] = {0, 0};
     int block_threads[2] = {0, 0}, block_grid[2] = {0, 0}, block_dcap[2] = {0, 0};
+    std::vector<BJob> hubs;  // jobs with a hub triangle to build before the counting kernels
 };
 
 // one (symmetric graph, 4-cycle app) job of a wedge-engine launch (global start-vertex index space)
@@ -246,7 +248,10 @@ int wedge_workers(uint32_t max_n);
 size_t wedge_arena_bytes(int n_jobs, uint64_t n_total, int workers, uint32_t max_n);
 khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunch *wl, cudaStream_t s);
 khz_status wedge_enqueue(const WedgeLaunch &wl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
-size_t bitmap_arena_bytes(int n_jobs, uint64_t list_cap);
+// rows of the hub triangle for a job on an oriented graph of n vertices and m edges under the
+// configured setting (0 = auto, < 0 = none)
+uint32_t bitmap_hub_rows(int cfg_rows, uint32_t n, uint64_t m);
+size_t bitmap_arena_bytes(const std::vector<BJob> &jobs, uint64_t list_cap);
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
                           int warp_max, Arena *arena, BitmapLaunch *bl, cudaStream_t s);
 khz_status bitmap_enqueue(const BitmapLaunch &bl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);

@@ -82,7 +82,7 @@ class Config(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("want_algo_bytes", ctypes.c_int32),
                 ("dfs_warps_per_sm", ctypes.c_int32), ("dfs_chunk", ctypes.c_int32),
                 ("bitmap_warp_max", ctypes.c_int32), ("bitmap_block_warps", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 10)]
+                ("bitmap_hub_rows", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
 
 
 class ServerStats(ctypes.Structure):
