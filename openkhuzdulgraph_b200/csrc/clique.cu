@@ -330,22 +330,50 @@ __device__ __forceinline__ void deal_flush(const Local &g, int K, const uint64_t
     }
 }
 
-// Count over rows [row_begin, d) with stride row_step for a k-clique job: one unit per word of
-// the row's non-zero extent, 32 words at a time.
+// Count over rows [row_begin, d) with stride row_step for a k-clique job.  The items (i, j) of a
+// row word are appended to the warp's 64-entry ring in shared memory (lane l writes the item of
+// bit l at its rank among the word's set bits), and each time 32 items are pending the lanes
+// take one each: items of consecutive words and rows pack into full batches.
+constexpr int kRing = 64;
 template <bool STATS, int KMAX>
-__device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, Acc &a) {
+__device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, uint32_t *ring,
+                           Acc &a) {
     const int lane = (int)lane_id();
-    int pc = 0, my_i = 0, my_j = 0;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t head = 0, tail = 0;  // ring positions (warp-uniform); pending items: tail - head < 32
     for (int i = row_begin; i < g.d; i += row_step) {
         const uint32_t *ri = g.rows + (size_t)i * g.S;
         const int lo = g.rlo[i], hi = g.rhi[i];
         if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]));
-        for (int base = lo; base < hi; base += 32) {
-            const int w = base + lane;
-            deal_units<STATS, KMAX>(g, K, off, i, w, w < hi ? ri[w] : 0u, pc, my_i, my_j, a);
+        for (int w = lo; w < hi; ++w) {
+            const uint32_t bits = ri[w];
+            const uint32_t c = __popc(bits);
+            if (lane == 0) {
+                a.t3 += c;
+                if (STATS) a.bytes += 4ull * c;
+                if (K == 3) a.cnt += c;
+            }
+            if (K == 3) continue;
+            if ((bits >> lane) & 1u)
+                ring[(tail + __popc(bits & below)) & (kRing - 1)] = ((uint32_t)i << 16) | (uint32_t)((w << 5) + lane);
+            tail += c;
+            if (tail - head >= 32) {
+                __syncwarp();
+                const uint32_t it = ring[(head + lane) & (kRing - 1)];
+                __syncwarp();
+                head += 32;
+                if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+                else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+            }
         }
     }
-    deal_flush<STATS, KMAX>(g, K, off, pc, my_i, my_j, a);
+    __syncwarp();
+    if (K > 3 && (uint32_t)lane < tail - head) {
+        const uint32_t it = ring[(head + lane) & (kRing - 1)];
+        if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+        else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+    }
+    __syncwarp();
 }
 
 // The same over all rows of a warp-tier start vertex (W = 2 words per row): 16 rows per round.
@@ -486,11 +514,13 @@ __host__ __device__ __forceinline__ int block_logt(int dcap) {
     while ((1 << l) < per * dcap) ++l;
     return l;
 }
-__host__ __device__ __forceinline__ size_t block_smem(int dcap) {
+__host__ __device__ __forceinline__ size_t block_rows_words(int dcap) {
+    return (size_t)((dcap + 31) & ~31) * ((size_t)((dcap + 31) / 32) | 1);
+}
+__host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads) {
     const size_t dp = (size_t)((dcap + 31) & ~31);
     const size_t t = (size_t)1 << block_logt(dcap);
-    const size_t w = (size_t)((dcap + 31) / 32) | 1;
-    return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + dp * w * 4;
+    return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + block_rows_words(dcap) * 4 + (size_t)(threads / 32) * kRing * 4;
 }
 
 // Block tier: one block per start vertex; the list holds global start-vertex indices, heaviest
@@ -515,6 +545,7 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
     g.logt = logt;
     const int warps = blockDim.x >> 5;
     const int wib = threadIdx.x >> 5;
+    uint32_t *ring = g.rows + block_rows_words(dcap) + (size_t)wib * kRing;
     const unsigned int n_list = *list_len;
     Acc a = {0, 0, 0, 0};
     int cur_job = -1;
@@ -557,7 +588,7 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
         __syncthreads();
         row_extents(g, threadIdx.x, blockDim.x);
         __syncthreads();
-        count_rows<STATS, KMAX>(g, jobs[j].k, off, wib, warps, a);
+        count_rows<STATS, KMAX>(g, jobs[j].k, off, wib, warps, ring, a);
         __syncthreads();
     }
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
@@ -714,12 +745,13 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     const int dcaps[2] = {kMidMax, L.large_dcap};
     const int threads[2] = {256, 1024};
     for (int t = 0; t < 2; ++t) {
-        const size_t smem = block_smem(dcaps[t]);
+        const size_t smem = block_smem(dcaps[t], threads[t]);
         auto kern = stats ? (L.kmax == 5 ? clique_block_kernel<true, 5> : clique_block_kernel<true, 4>)
                           : (L.kmax == 5 ? clique_block_kernel<false, 5> : clique_block_kernel<false, 4>);
         // the attribute is per kernel, shared by every prepared launch: always allow the largest
         // footprint so launches prepared earlier with more shared memory stay valid
-        KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)block_smem(kBlockMax)));
+        KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)block_smem(kBlockMax, 1024)));
         int per_sm = 0;
         KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
         L.block_smem[t] = smem;

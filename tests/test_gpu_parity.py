@@ -333,6 +333,42 @@ def test_bitmap_large_tier_matches_oracle(khz_ctx):
         og.free()
 
 
+@pytest.mark.parametrize("hub_rows", [64, 992, 1 << 30])
+def test_hub_triangle_matches_oracle(graphs, khz_ctx, hub_rows):
+    """Rows of hub vertices read from the hub adjacency triangle (here forced on small graphs, up
+    to every vertex a hub) give the oracle's counts, NumExtensions and algorithmic bytes."""
+    from openkhuzdulgraph_b200 import khz
+    canon, n = orc.er(1500, 250000, seed=5)
+    dense = orc.symmetrize(canon)
+    cases = [(spec["name"], n_, sym) for spec, n_, sym, _, _, _ in graphs] + [("er_n1500_dense", n, dense)]
+    khz_ctx.set_config(engine=khz.ENGINE_BITMAP, want_algo_bytes=1, bitmap_hub_rows=hub_rows)
+    try:
+        for name, n_, sym in cases:
+            off, adj = orc.csr(sym, n_)
+            ooff, oadj, _ = orc.orient(off, adj)
+            og = khz_ctx.graph_from_edges(sym, n_, orient=True)
+            try:
+                for app in ["kautomine_triangle", "kautomine_four_clique", "kgraphpi_five_clique"]:
+                    got, st = khz_ctx.count(og, app)
+                    exp, ext, byt = orc.count(app, ooff, oadj)
+                    assert got == exp and st.num_extensions == ext and st.algo_bytes == byt, (name, app)
+            finally:
+                og.free()
+        # 3-motif on symmetric input: triangles of the oriented view through the same path
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO, want_algo_bytes=0, bitmap_hub_rows=hub_rows)
+        g = khz_ctx.graph_from_edges(dense, n)
+        try:
+            off, adj = orc.csr(dense, n)
+            for app in ["kautomine_three_motif", "kgraphpi_three_motif"]:
+                got, st = khz_ctx.count(g, app)
+                exp, ext, _ = orc.count(app, off, adj)
+                assert got == exp and st.num_extensions == ext, app
+        finally:
+            g.free()
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO, want_algo_bytes=0, bitmap_hub_rows=0)
+
+
 def test_bitmap_overflow_tier_complete_graph(khz_ctx):
     """K_1250: out-degrees up to 1249 exceed the block tier, so the heaviest start vertices go to
     the DFS engine; counts and NumExtensions follow from binomial coefficients."""
