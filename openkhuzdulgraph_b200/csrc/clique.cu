@@ -31,7 +31,7 @@ namespace {
 
 constexpr int kWarpMax = 64;          // warp tier: d <= 64 -> 2 words per row
 constexpr int kMidMax = 256;          // mid block tier
-constexpr int kBlockMax = 1216;       // large block tier: 1216 rows x 39 words = 185 KiB (+ hash 24 KiB)
+constexpr int kBlockMax = 1216;       // large block tier: 1216 rows x 38 words = 180 KiB (+ hash 24 KiB)
 
 // position of the n-th (0-based) set bit of x; x must have more than n set bits
 __device__ __forceinline__ int nth_set_bit(uint32_t x, int n) {
@@ -79,16 +79,20 @@ __host__ __device__ __forceinline__ uint64_t hub_row_offset(uint32_t h, uint32_t
 //   c[d]            the candidates (sorted vertex ids)
 //   hkey/hidx[T]    open-addressing hash of c: vertex id -> position (T = 2^logt >= 2d)
 //   rows[d * S]     bit j of row i set iff c[j] in N+(c[i])   (only j > i); W = ceil(d / 32)
-//                   words per row at an odd stride S = W | 1, so that lanes reading the same
-//                   word offset of different rows hit different shared-memory banks
-//   rlo/rhi[d]      first / one-past-last non-zero word of each row
+//                   32-bit words, read as W64 = ceil(d / 64) 64-bit words by the counting loops,
+//                   at a stride of S = 2 (W64 | 1) 32-bit words: odd in 64-bit words, so that
+//                   lanes reading the same word offset of different rows hit different banks
+//   rlo/rhi[d]      first / one-past-last non-zero 64-bit word of each row
 struct Local {
     uint32_t *c;
     uint32_t *hkey;
     uint16_t *hidx;
     uint32_t *rows;
     uint16_t *rlo, *rhi;
-    int d, W, S, logt;
+    int d, W, W64, S, logt;
+    __device__ __forceinline__ const uint64_t *row64(int i) const {
+        return reinterpret_cast<const uint64_t *>(rows + (size_t)i * S);
+    }
     const uint32_t *hub;  // the job's hub triangle, or null
     uint32_t hub_base, hub_wh;
     __device__ __forceinline__ uint32_t slot(uint32_t x) const { return (x * 0x9E3779B1u) >> (32 - logt); }
@@ -223,30 +227,30 @@ __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, con
 // first / one-past-last non-zero word of rows [tid, d) step nthr
 __device__ __forceinline__ void row_extents(const Local &g, int tid, int nthr) {
     for (int i = tid; i < g.d; i += nthr) {
-        const uint32_t *r = g.rows + (size_t)i * g.S;
-        int lo = g.W, hi = 0;
-        for (int w = (i + 1) >> 5; w < g.W; ++w) {
+        const uint64_t *r = g.row64(i);
+        int lo = g.W64, hi = 0;
+        for (int w = (i + 1) >> 6; w < g.W64; ++w) {
             if (r[w]) {
                 lo = min(lo, w);
                 hi = w + 1;
             }
         }
-        g.rlo[i] = (uint16_t)(hi == 0 ? g.W : lo);
+        g.rlo[i] = (uint16_t)(hi == 0 ? g.W64 : lo);
         g.rhi[i] = (uint16_t)hi;
     }
 }
 
 template <int K, bool STATS>
 __device__ __forceinline__ void process_item(const Local &g, int i, int j, const uint64_t *off, Acc &a) {
-    const uint32_t *ri = g.rows + (size_t)i * g.S;
-    const uint32_t *rj = g.rows + (size_t)j * g.S;
+    const uint64_t *ri = g.row64(i);
+    const uint64_t *rj = g.row64(j);
     const int lo = max((int)g.rlo[i], (int)g.rlo[j]);
     const int hi = min((int)g.rhi[i], (int)g.rhi[j]);
     uint32_t s = 0;
-    for (int w = lo; w < hi; ++w) s += __popc(ri[w] & rj[w]);
+    for (int w = lo; w < hi; ++w) s += __popcll(ri[w] & rj[w]);
     if (STATS) {
         uint32_t pi = 0;
-        for (int w = g.rlo[i]; w < g.rhi[i]; ++w) pi += __popc(ri[w]);
+        for (int w = g.rlo[i]; w < g.rhi[i]; ++w) pi += __popcll(ri[w]);
         a.bytes += 4ull * ((uint64_t)pi + odeg(off, g.c[j]) + s);
     }
     if (K == 4) {
@@ -255,15 +259,15 @@ __device__ __forceinline__ void process_item(const Local &g, int i, int j, const
     }
     a.t4 += s;
     for (int w1 = lo; w1 < hi; ++w1) {
-        uint32_t m = ri[w1] & rj[w1];
+        uint64_t m = ri[w1] & rj[w1];
         while (m) {
-            const int l = (w1 << 5) + __ffs(m) - 1;
+            const int l = (w1 << 6) + __ffsll((long long)m) - 1;
             m &= m - 1;
-            const uint32_t *rl = g.rows + (size_t)l * g.S;
+            const uint64_t *rl = g.row64(l);
             const int lo3 = max(lo, (int)g.rlo[l]);
             const int hi3 = min(hi, (int)g.rhi[l]);
             uint32_t t = 0;
-            for (int w = lo3; w < hi3; ++w) t += __popc(ri[w] & rj[w] & rl[w]);
+            for (int w = lo3; w < hi3; ++w) t += __popcll(ri[w] & rj[w] & rl[w]);
             a.cnt += t;
             if (STATS) a.bytes += 4ull * ((uint64_t)s + odeg(off, g.c[l]) + t);
         }
@@ -342,28 +346,35 @@ __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_b
     const uint32_t below = (1u << lane) - 1u;
     uint32_t head = 0, tail = 0;  // ring positions (warp-uniform); pending items: tail - head < 32
     for (int i = row_begin; i < g.d; i += row_step) {
-        const uint32_t *ri = g.rows + (size_t)i * g.S;
+        const uint64_t *ri = g.row64(i);
         const int lo = g.rlo[i], hi = g.rhi[i];
         if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]));
         for (int w = lo; w < hi; ++w) {
-            const uint32_t bits = ri[w];
-            const uint32_t c = __popc(bits);
+            const uint64_t bits = ri[w];
+            const uint32_t b0 = (uint32_t)bits, b1 = (uint32_t)(bits >> 32);
+            const uint32_t c0 = __popc(b0), c = c0 + __popc(b1);
             if (lane == 0) {
                 a.t3 += c;
                 if (STATS) a.bytes += 4ull * c;
                 if (K == 3) a.cnt += c;
             }
             if (K == 3) continue;
-            if ((bits >> lane) & 1u)
-                ring[(tail + __popc(bits & below)) & (kRing - 1)] = ((uint32_t)i << 16) | (uint32_t)((w << 5) + lane);
-            tail += c;
-            if (tail - head >= 32) {
-                __syncwarp();
-                const uint32_t it = ring[(head + lane) & (kRing - 1)];
-                __syncwarp();
-                head += 32;
-                if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
-                else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+            // the two 32-bit halves in turn, a batch taken after each: at most 63 items pending
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const uint32_t b = half ? b1 : b0;
+                if ((b >> lane) & 1u)
+                    ring[(tail + __popc(b & below)) & (kRing - 1)] =
+                        ((uint32_t)i << 16) | (uint32_t)((w << 6) + (half << 5) + lane);
+                tail += half ? c - c0 : c0;
+                if (tail - head >= 32) {
+                    __syncwarp();
+                    const uint32_t it = ring[(head + lane) & (kRing - 1)];
+                    __syncwarp();
+                    head += 32;
+                    if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+                    else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+                }
             }
         }
     }
@@ -433,10 +444,11 @@ __global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restr
                                                           unsigned long long *queue, uint64_t *rows_out,
                                                           uint64_t *phase_bytes) {
     constexpr int W = kWarpMax / 32;
-    constexpr int S = W | 1;
+    constexpr int W64 = kWarpMax / 64;
+    constexpr int S = 2 * (W64 | 1);
     constexpr int T = 1 << kWarpHashLog;
     __shared__ uint32_t s_c[8][kWarpMax];
-    __shared__ uint32_t s_rows[8][kWarpMax * S];
+    __shared__ uint64_t s_rows[8][kWarpMax * S / 2];
     __shared__ uint32_t s_hkey[8][T];
     __shared__ uint16_t s_hidx[8][T];
     __shared__ uint16_t s_rlo[8][kWarpMax], s_rhi[8][kWarpMax];
@@ -444,12 +456,13 @@ __global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restr
     const int wib = threadIdx.x >> 5;
     Local g;
     g.c = s_c[wib];
-    g.rows = s_rows[wib];
+    g.rows = reinterpret_cast<uint32_t *>(s_rows[wib]);
     g.hkey = s_hkey[wib];
     g.hidx = s_hidx[wib];
     g.rlo = s_rlo[wib];
     g.rhi = s_rhi[wib];
     g.W = W;
+    g.W64 = W64;
     g.S = S;
     g.logt = kWarpHashLog;
     Acc a = {0, 0, 0, 0};
@@ -515,7 +528,7 @@ __host__ __device__ __forceinline__ int block_logt(int dcap) {
     return l;
 }
 __host__ __device__ __forceinline__ size_t block_rows_words(int dcap) {
-    return (size_t)((dcap + 31) & ~31) * ((size_t)((dcap + 31) / 32) | 1);
+    return (size_t)((dcap + 31) & ~31) * 2 * ((size_t)((dcap + 63) / 64) | 1);
 }
 __host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads) {
     const size_t dp = (size_t)((dcap + 31) & ~31);
@@ -576,7 +589,8 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
         g.hub_wh = jobs[j].hub_rows >> 5;
         g.d = (int)odeg(off, v0);
         g.W = (g.d + 31) >> 5;
-        g.S = g.W | 1;
+        g.W64 = (g.d + 63) >> 6;
+        g.S = 2 * (g.W64 | 1);
         const uint64_t b0 = __ldg(off + v0);
         for (int t = threadIdx.x; t < g.d; t += blockDim.x) g.c[t] = __ldg(adj + b0 + t);
         for (int t = threadIdx.x; t < g.d * g.S; t += blockDim.x) g.rows[t] = 0;
