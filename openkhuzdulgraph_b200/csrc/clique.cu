@@ -387,6 +387,26 @@ __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_b
     __syncwarp();
 }
 
+// Rows of at most 8 words (the mid tier): one unit per 32-bit word, the words of 32 / wp rows per
+// round (wp = 4 or 8, a power of two >= W), dealt as in the warp tier; per-row work is spread
+// over the lanes instead of running row by row.
+template <bool STATS, int KMAX>
+__device__ void count_rows_units(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, Acc &a) {
+    const int lane = (int)lane_id();
+    const int lg = g.W <= 4 ? 2 : 3;
+    const int nrows = (g.d - row_begin + row_step - 1) / row_step;  // rows of this warp
+    int pc = 0, my_i = 0, my_j = 0;
+    for (int k0 = 0; k0 < nrows; k0 += 32 >> lg) {
+        const int k = k0 + (lane >> lg), w = lane & ((1 << lg) - 1);
+        const int i = row_begin + k * row_step;
+        const bool ok = k < nrows && w < g.W;
+        const uint32_t bits = ok ? g.rows[(size_t)i * g.S + w] : 0u;
+        if (STATS && ok && w == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]));
+        deal_units<STATS, KMAX>(g, K, off, i, w, bits, pc, my_i, my_j, a);
+    }
+    deal_flush<STATS, KMAX>(g, K, off, pc, my_i, my_j, a);
+}
+
 // The same over all rows of a warp-tier start vertex (W = 2 words per row): 16 rows per round.
 template <bool STATS, int KMAX>
 __device__ void count_rows_small(const Local &g, int K, const uint64_t *off, Acc &a) {
@@ -537,9 +557,14 @@ __host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads) {
 }
 
 // Block tier: one block per start vertex; the list holds global start-vertex indices, heaviest
-// degree bucket first, and its length is read from device memory.
-template <bool STATS, int KMAX>
-__global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ list,
+// degree bucket first, and its length is read from device memory.  The mid tier runs 256-thread
+// blocks, several per SM (registers capped for that), the large tier one 1024-thread block per SM
+// (its shared memory fills the SM).
+constexpr int kMidThreads = 256, kLargeThreads = 1024;
+constexpr int kMidMinBlocks = 5;
+template <bool STATS, int KMAX, int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : kMidMinBlocks)
+    clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ list,
                                     const unsigned int *__restrict__ list_len, int dcap, unsigned long long *queue,
                                     uint64_t *rows_out, uint64_t *phase_bytes) {
     extern __shared__ __align__(16) uint32_t smem[];
@@ -602,10 +627,23 @@ __global__ void clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, c
         __syncthreads();
         row_extents(g, threadIdx.x, blockDim.x);
         __syncthreads();
-        count_rows<STATS, KMAX>(g, jobs[j].k, off, wib, warps, ring, a);
+        if (g.W <= 8) count_rows_units<STATS, KMAX>(g, jobs[j].k, off, wib, warps, a);
+        else count_rows<STATS, KMAX>(g, jobs[j].k, off, wib, warps, ring, a);
         __syncthreads();
     }
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
+}
+
+using BlockKernel = void (*)(const BJob *, int, const uint32_t *, const unsigned int *, int, unsigned long long *,
+                             uint64_t *, uint64_t *);
+template <int THREADS>
+BlockKernel block_kernel_of(bool stats, int kmax) {
+    return stats ? (kmax == 5 ? clique_block_kernel<true, 5, THREADS> : clique_block_kernel<true, 4, THREADS>)
+                 : (kmax == 5 ? clique_block_kernel<false, 5, THREADS> : clique_block_kernel<false, 4, THREADS>);
+}
+// tier 0: mid, tier 1: large
+BlockKernel block_kernel(bool stats, int kmax, int tier) {
+    return tier == 0 ? block_kernel_of<kMidThreads>(stats, kmax) : block_kernel_of<kLargeThreads>(stats, kmax);
 }
 
 // The hub triangle of one job (zeroed beforehand): one warp per hub row.
@@ -757,17 +795,20 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     L.has_mid = max_outdeg > L.warp_max;
     L.has_large = max_outdeg > (uint32_t)kMidMax;
     const int dcaps[2] = {kMidMax, L.large_dcap};
-    const int threads[2] = {256, 1024};
+    const int threads[2] = {kMidThreads, kLargeThreads};
     for (int t = 0; t < 2; ++t) {
         const size_t smem = block_smem(dcaps[t], threads[t]);
-        auto kern = stats ? (L.kmax == 5 ? clique_block_kernel<true, 5> : clique_block_kernel<true, 4>)
-                          : (L.kmax == 5 ? clique_block_kernel<false, 5> : clique_block_kernel<false, 4>);
+        const BlockKernel kern = block_kernel(stats, L.kmax, t);
         // the attribute is per kernel, shared by every prepared launch: always allow the largest
         // footprint so launches prepared earlier with more shared memory stay valid
         KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)block_smem(kBlockMax, 1024)));
         int per_sm = 0;
         KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
+        if (per_sm < 1) {
+            set_error("bitmap block kernel does not fit an SM (%d threads, %zu bytes of shared memory)", threads[t], smem);
+            return KHZ_ERR_CUDA;
+        }
         L.block_smem[t] = smem;
         L.block_threads[t] = threads[t];
         L.block_grid[t] = L.sms * std::max(per_sm, 1);
@@ -821,8 +862,7 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
         const uint32_t *list = t == 0 ? L.mid_list : L.large_list;
         const unsigned int *len = L.cnt + (t == 0 ? kCntMidLen : kCntLargeLen);
         mark(1 + t, true);
-        auto bk = L.stats ? (L.kmax == 5 ? clique_block_kernel<true, 5> : clique_block_kernel<true, 4>)
-                          : (L.kmax == 5 ? clique_block_kernel<false, 5> : clique_block_kernel<false, 4>);
+        const BlockKernel bk = block_kernel(L.stats, L.kmax, t);
         bk<<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(L.d_jobs, L.n_jobs, list, len, L.block_dcap[t],
                                                                        &L.queues[1 + t], d_rows, pb(1 + t));
         KHZ_CUDA(cudaGetLastError());
