@@ -335,48 +335,48 @@ __device__ __forceinline__ void deal_flush(const Local &g, int K, const uint64_t
 }
 
 // Count over rows [row_begin, d) with stride row_step for a k-clique job.  The items (i, j) of a
-// row word are appended to the warp's 64-entry ring in shared memory (lane l writes the item of
-// bit l at its rank among the word's set bits), and each time 32 items are pending the lanes
-// take one each: items of consecutive words and rows pack into full batches.
-constexpr int kRing = 64;
+// 64-bit row word are appended to the warp's kRing-entry ring in shared memory (lane l writes the
+// items of bits l and 32 + l at their ranks among the word's set bits), and while 32 items are
+// pending the lanes take one each: items of consecutive words and rows pack into full batches.
+// The triangles through the rows (NumExtensions) are the number of items dealt.
+constexpr int kRing = 128;
 template <bool STATS, int KMAX>
 __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_begin, int row_step, uint32_t *ring,
                            Acc &a) {
     const int lane = (int)lane_id();
-    const uint32_t below = (1u << lane) - 1u;
-    uint32_t head = 0, tail = 0;  // ring positions (warp-uniform); pending items: tail - head < 32
+    const uint32_t lanebit = 1u << lane, below = lanebit - 1u;
+    uint32_t head = 0, tail = 0;  // ring positions (warp-uniform); pending items tail - head < 32
     for (int i = row_begin; i < g.d; i += row_step) {
         const uint64_t *ri = g.row64(i);
         const int lo = g.rlo[i], hi = g.rhi[i];
         if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]));
+        const uint32_t ibase = ((uint32_t)i << 16) + (uint32_t)lane;
         for (int w = lo; w < hi; ++w) {
             const uint64_t bits = ri[w];
             const uint32_t b0 = (uint32_t)bits, b1 = (uint32_t)(bits >> 32);
-            const uint32_t c0 = __popc(b0), c = c0 + __popc(b1);
-            if (lane == 0) {
-                a.t3 += c;
-                if (STATS) a.bytes += 4ull * c;
-                if (K == 3) a.cnt += c;
+            const uint32_t c0 = __popc(b0);
+            if (K == 3) {
+                tail += c0 + __popc(b1);
+                continue;
             }
-            if (K == 3) continue;
-            // the two 32-bit halves in turn, a batch taken after each: at most 63 items pending
-#pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                const uint32_t b = half ? b1 : b0;
-                if ((b >> lane) & 1u)
-                    ring[(tail + __popc(b & below)) & (kRing - 1)] =
-                        ((uint32_t)i << 16) | (uint32_t)((w << 6) + (half << 5) + lane);
-                tail += half ? c - c0 : c0;
-                if (tail - head >= 32) {
-                    __syncwarp();
-                    const uint32_t it = ring[(head + lane) & (kRing - 1)];
-                    __syncwarp();
-                    head += 32;
-                    if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
-                    else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
-                }
+            const uint32_t item = ibase + ((uint32_t)w << 6);
+            if (b0 & lanebit) ring[(tail + __popc(b0 & below)) & (kRing - 1)] = item;
+            if (b1 & lanebit) ring[(tail + c0 + __popc(b1 & below)) & (kRing - 1)] = item + 32;
+            tail += c0 + __popc(b1);
+            while (tail - head >= 32) {
+                __syncwarp();
+                const uint32_t it = ring[(head + lane) & (kRing - 1)];
+                __syncwarp();
+                head += 32;
+                if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+                else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
             }
         }
+    }
+    if (lane == 0) {
+        a.t3 += tail;
+        if (STATS) a.bytes += 4ull * tail;
+        if (K == 3) a.cnt += tail;
     }
     __syncwarp();
     if (K > 3 && (uint32_t)lane < tail - head) {
@@ -541,11 +541,11 @@ __global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restr
 // shared-memory footprint of a block-tier launch serving out-degrees up to dcap
 __host__ __device__ __forceinline__ int block_logt(int dcap) {
     // hash slots per candidate: 8 (almost every miss ends at the first slot) where shared memory
-    // allows, 2 for the largest candidate sets
+    // allows, 2 for larger candidate sets (at most 2048 slots, so that the large tier fits an SM)
     const int per = dcap <= kMidMax ? 8 : 2;
     int l = 5;
     while ((1 << l) < per * dcap) ++l;
-    return l;
+    return (dcap <= kMidMax || l <= 11) ? l : 11;  // <= 2048 slots: >= 1.68 per candidate up to kBlockMax
 }
 __host__ __device__ __forceinline__ size_t block_rows_words(int dcap) {
     return (size_t)((dcap + 31) & ~31) * 2 * ((size_t)((dcap + 63) / 64) | 1);
