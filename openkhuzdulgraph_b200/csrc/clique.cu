@@ -247,7 +247,17 @@ __device__ __forceinline__ void process_item(const Local &g, int i, int j, const
     const int lo = max((int)g.rlo[i], (int)g.rlo[j]);
     const int hi = min((int)g.rhi[i], (int)g.rhi[j]);
     uint32_t s = 0;
-    for (int w = lo; w < hi; ++w) s += __popcll(ri[w] & rj[w]);
+    {
+        // the hot loop with 32-bit shared-window addresses stepped by one 64-bit word
+        const uint32_t sb = (uint32_t)__cvta_generic_to_shared(g.rows);
+        uint32_t ai = sb + (uint32_t)(i * g.S + 2 * lo) * 4u, aj = sb + (uint32_t)(j * g.S + 2 * lo) * 4u;
+        for (int w = lo; w < hi; ++w, ai += 8, aj += 8) {
+            uint64_t x, y;
+            asm("ld.shared.u64 %0, [%1];" : "=l"(x) : "r"(ai));
+            asm("ld.shared.u64 %0, [%1];" : "=l"(y) : "r"(aj));
+            s += __popcll(x & y);
+        }
+    }
     if (STATS) {
         uint32_t pi = 0;
         for (int w = g.rlo[i]; w < g.rhi[i]; ++w) pi += __popcll(ri[w]);
