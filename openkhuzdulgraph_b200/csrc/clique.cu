@@ -752,6 +752,7 @@ uint32_t bitmap_hub_rows(int cfg_rows, uint32_t n, uint64_t m) {
 }
 
 static size_t hub_words(uint32_t rows) { return rows ? (size_t)hub_row_offset(rows, rows >> 5) : 0; }
+size_t bitmap_hub_bytes(uint32_t rows) { return sizeof(uint32_t) * hub_words(rows); }
 
 size_t bitmap_arena_bytes(const std::vector<BJob> &jobs, uint64_t list_cap) {
     size_t b = Arena::round(sizeof(BJob) * std::max<size_t>(jobs.size(), 1)) +

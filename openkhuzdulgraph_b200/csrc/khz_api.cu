@@ -408,7 +408,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             P->engine = KHZ_ENGINE_BITMAP;
         } else if (engine == KHZ_ENGINE_WEDGE) {
             const Graph &g = *get_graph(ctx, jobs[i].graph);
-            wjobs.push_back(WJob{g.off, g.adj, g.n, 0, wbase, (uint32_t)i, 0});
+            wjobs.push_back(WJob{g.off, g.adj, g.n, g.max_degree, wbase, (uint32_t)i, 0});
             wbase += g.n;
             ext_add[i] = (uint64_t)g.n + g.m / 2;  // depth 0 and every undirected edge once at depth 1
             if (P->engine == KHZ_ENGINE_DFS) P->engine = KHZ_ENGINE_WEDGE;
@@ -421,8 +421,6 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     P->has_bitmap = !bjobs.empty();
     P->has_dfs = !djobs.empty();
     P->has_wedge = !wjobs.empty();
-    uint32_t wmax_n = 0;
-    for (const auto &w : wjobs) wmax_n = std::max(wmax_n, w.n);
     const int warp_max = ctx->cfg.bitmap_warp_max == 32 ? 32 : 64;
     // every listed start vertex has more than warp_max out-edges
     const uint64_t list_cap = std::min<uint64_t>(std::max<uint64_t>(vbase, 1), bm_entries / (warp_max + 1) + 1);
@@ -431,7 +429,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
                    Arena::round(sizeof(uint64_t) * n) + Arena::round(sizeof(unsigned int)) +
                    Arena::round(sizeof(uint64_t) * kPhases);
     if (P->has_bitmap) bytes += bitmap_arena_bytes(bjobs, list_cap);
-    if (P->has_wedge) bytes += wedge_arena_bytes((int)wjobs.size(), wbase, wedge_workers(wmax_n), wmax_n);
+    if (P->has_wedge) bytes += wedge_arena_bytes((int)wjobs.size(), wbase);
     if (!mjobs.empty()) bytes += Arena::round(sizeof(MJob) * mjobs.size());
     if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
     P->slot_words = P->has_dfs ? dfs_slot_words(ctx->cfg.dfs_warps_per_sm, slot_cap) : 0;
@@ -633,12 +631,12 @@ khz_status serve_footprint(khz_server *sv, khz_graph h, int app, uint64_t *bytes
     uint64_t b = 1ull << 16;
     const int eng = pick_engine(ctx->cfg, def, app, *g);
     if (eng == KHZ_ENGINE_WEDGE) {
-        b += 3 * 4 * (uint64_t)g->n + 4ull * wedge_workers(g->n) * g->n;
+        b += 3 * 4 * (uint64_t)g->n;
     } else if (eng == KHZ_ENGINE_BITMAP) {
         Graph *og = nullptr;
         khz_status st = oriented_of(ctx, h, &og, nullptr);  // orient once, before any timing matters
         if (st) return st;
-        b += 2 * 4 * (og->m / 33 + 1);
+        b += 2 * 4 * (og->m / 33 + 1) + bitmap_hub_bytes(bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m));
         if (og->max_degree > bitmap_block_max_degree())
             b += 4 * dfs_slot_words(ctx->cfg.dfs_warps_per_sm, og->max_degree);
     } else {

@@ -150,7 +150,7 @@ struct WJob {
     const uint64_t *off;
     const uint32_t *adj;
     uint32_t n;
-    uint32_t pad;
+    uint32_t max_deg;
     uint64_t vbase;
     uint32_t out_row;
     uint32_t pad2;
@@ -160,12 +160,11 @@ struct WedgeLaunch {
     const WJob *d_jobs = nullptr;
     int n_jobs = 0;
     uint64_t n_total = 0, list_cap = 0;
-    uint32_t max_n = 0;
-    uint32_t *lists = nullptr;   // warp, block and global tier lists (list_cap each)
+    uint32_t *lists = nullptr;   // warp, block and window tier lists (list_cap each)
     unsigned int *cnt = nullptr;
     unsigned long long *queues = nullptr;
-    uint32_t *dense = nullptr;   // workers * max_n counters, kept zeroed
-    int workers = 0, sms = 0;
+    bool wide = false;           // 32-bit window counters (some degree reaches 65535)
+    int sms = 0;
 };
 
 // device resources and launch shape of one DFS-engine launch
@@ -244,13 +243,13 @@ khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_p
 // DfsJob::min_deg.  No host synchronisation in bitmap_enqueue.
 // Wedge engine (4-cycle on symmetric graphs): adds each job's count (row[0]) and its level-2
 // NumExtensions (row[6]); no host synchronisation in wedge_enqueue.
-int wedge_workers(uint32_t max_n);
-size_t wedge_arena_bytes(int n_jobs, uint64_t n_total, int workers, uint32_t max_n);
+size_t wedge_arena_bytes(int n_jobs, uint64_t n_total);
 khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunch *wl, cudaStream_t s);
 khz_status wedge_enqueue(const WedgeLaunch &wl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 // rows of the hub triangle for a job on an oriented graph of n vertices and m edges under the
 // configured setting (0 = auto, < 0 = none)
 uint32_t bitmap_hub_rows(int cfg_rows, uint32_t n, uint64_t m);
+size_t bitmap_hub_bytes(uint32_t rows);
 size_t bitmap_arena_bytes(const std::vector<BJob> &jobs, uint64_t list_cap);
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
                           int warp_max, Arena *arena, BitmapLaunch *bl, cudaStream_t s);

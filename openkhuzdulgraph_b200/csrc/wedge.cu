@@ -11,7 +11,9 @@
 //
 // Tiers by the number of wedges of v0 (an upper bound on distinct endpoints): one warp with a
 // 512-slot shared hash (<= 384 wedges), one block with an 8192-slot shared hash (<= 6144), or one
-// block with a dense counter array in global memory (reset by re-walking the wedges).
+// 1024-thread block with dense counters in shared memory over a window of endpoint ids (106496
+// 16-bit counters, or 53248 32-bit ones when a degree reaches 65535), the endpoints v2 > v0 taken
+// one window at a time; each neighbour list's part inside the window is found by binary search.
 #include <cuda_runtime.h>
 
 #include "khz_internal.cuh"
@@ -24,6 +26,8 @@ constexpr uint32_t kEmptyKey = 0xffffffffu;
 constexpr int kWarpSlots = 512, kWarpWedges = 384;
 constexpr int kBlockSlots = 8192, kBlockWedges = 6144;
 constexpr int kBlockThreads = 512;
+constexpr int kWinThreads = 1024;
+constexpr uint32_t kWinWords = 53248;  // 208 KiB of shared counters per block
 
 __device__ __forceinline__ int wjob_of(const WJob *jobs, int n_jobs, uint64_t gv) {
     int lo = 0, hi = n_jobs - 1;
@@ -78,6 +82,25 @@ __global__ void wedge_classify_kernel(const WJob *__restrict__ jobs, int n_jobs,
     }
 }
 
+// The part of the sorted list L[0, len) inside [lo, hi), widened to whole gaps between 32 evenly
+// spaced splitters read in one warp-wide load (instead of two binary searches of dependent loads):
+// entries outside [lo, hi) in the returned range are filtered by the caller.
+struct Span {
+    uint32_t begin, end;
+};
+__device__ __forceinline__ Span splitter_span(const uint32_t *__restrict__ L, uint32_t len, uint32_t lo, uint32_t hi) {
+    const uint32_t lane = lane_id();
+    const uint64_t step = ((uint64_t)len + 31) >> 5;
+    const uint64_t sidx = lane * step;
+    const uint32_t sp = sidx < len ? __ldg(L + sidx) : kEmptyKey;
+    const uint64_t k_lo = __popc(__ballot_sync(kFull, sp < lo));
+    const uint64_t k_hi = __popc(__ballot_sync(kFull, sp < hi));
+    Span r;
+    r.begin = (uint32_t)(k_lo == 0 ? 0 : (k_lo - 1) * step + 1);
+    r.end = (uint32_t)min((uint64_t)len, k_hi * step);
+    return r;
+}
+
 // Walk the wedges (v0, w, v2) of one start vertex with the calling threads: warp `wid` of `nw`
 // takes every nw-th w, its lanes take consecutive v2.  f(v2) is called once per wedge.
 template <typename F>
@@ -87,9 +110,13 @@ __device__ __forceinline__ void walk_wedges(const WJob &J, uint32_t v0, int wid,
     const uint32_t start = upper_bound_u32(J.adj + b, 0, (uint32_t)(e - b), v0);
     for (uint64_t i = b + start + wid; i < e; i += nw) {
         const uint32_t w = J.adj[i];
-        const uint64_t wb = J.off[w], we = J.off[w + 1];
-        const uint32_t s2 = upper_bound_u32(J.adj + wb, 0, (uint32_t)(we - wb), v0);
-        for (uint64_t k = wb + s2 + lane; k < we; k += 32) f(__ldg(J.adj + k));
+        const uint64_t wb = J.off[w];
+        const uint32_t len = (uint32_t)(J.off[w + 1] - wb);
+        const Span sp = splitter_span(J.adj + wb, len, v0 + 1, kEmptyKey);
+        for (uint64_t k = wb + sp.begin + lane; k < wb + sp.end; k += 32) {
+            const uint32_t v2 = __ldg(J.adj + k);
+            if (v2 > v0) f(v2);
+        }
     }
 }
 
@@ -170,15 +197,18 @@ __global__ void __launch_bounds__(kBlockThreads) wedge_block_kernel(const WJob *
     if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
 }
 
-// one block per heavy start vertex; `dense` holds one zeroed counter array of max_n words per
-// block, left zeroed after each start vertex by walking its wedges again
-__global__ void __launch_bounds__(kBlockThreads) wedge_global_kernel(const WJob *__restrict__ jobs, int n_jobs,
-                                                                     const uint32_t *__restrict__ list,
-                                                                     const unsigned int *__restrict__ list_len,
-                                                                     unsigned long long *queue, uint32_t *dense,
-                                                                     uint32_t max_n, uint64_t *rows) {
+// One block per heavy start vertex: the endpoints v2 in (v0, n) are counted one window of `span`
+// ids at a time in shared memory (16-bit counters packed two to a word unless WIDE: a count is at
+// most the graph's largest degree).
+template <bool WIDE>
+__global__ void __launch_bounds__(kWinThreads, 1) wedge_window_kernel(const WJob *__restrict__ jobs, int n_jobs,
+                                                                      const uint32_t *__restrict__ list,
+                                                                      const unsigned int *__restrict__ list_len,
+                                                                      unsigned long long *queue, uint64_t *rows) {
+    extern __shared__ __align__(16) uint32_t win[];
     __shared__ uint64_t s_gv;
-    uint32_t *cnt = dense + (size_t)blockIdx.x * max_n;
+    constexpr uint64_t span = WIDE ? kWinWords : 2ull * kWinWords;
+    const unsigned lane = lane_id();
     const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const unsigned int n_list = *list_len;
     uint64_t acc = 0;
@@ -196,30 +226,42 @@ __global__ void __launch_bounds__(kBlockThreads) wedge_global_kernel(const WJob 
             if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
             cur = j;
         }
-        const uint32_t v0 = (uint32_t)(gv - jobs[j].vbase);
-        walk_wedges(jobs[j], v0, wid, nw, [&](uint32_t v2) { acc += atomicAdd(&cnt[v2], 1u); });
-        __syncthreads();
-        walk_wedges(jobs[j], v0, wid, nw, [&](uint32_t v2) { cnt[v2] = 0; });
-        __syncthreads();
+        const WJob &J = jobs[j];
+        const uint32_t v0 = (uint32_t)(gv - J.vbase);
+        const uint64_t b = J.off[v0], e = J.off[v0 + 1];
+        const uint32_t start = upper_bound_u32(J.adj + b, 0, (uint32_t)(e - b), v0);
+        for (uint64_t base = (uint64_t)v0 + 1; base < J.n; base += span) {
+            for (uint32_t t = threadIdx.x; t < kWinWords; t += blockDim.x) win[t] = 0;
+            __syncthreads();
+            const uint64_t top = min((uint64_t)J.n, base + span);
+            for (uint64_t i = b + start + wid; i < e; i += nw) {
+                const uint32_t w = J.adj[i];
+                const uint64_t wb = J.off[w];
+                const uint32_t len = (uint32_t)(J.off[w + 1] - wb);
+                const Span sp = splitter_span(J.adj + wb, len, (uint32_t)base, (uint32_t)top);
+                for (uint64_t k = wb + sp.begin + lane; k < wb + sp.end; k += 32) {
+                    const uint32_t x = __ldg(J.adj + k) - (uint32_t)base;
+                    if (x >= (uint32_t)(top - base)) continue;  // outside the window (unsigned)
+                    if (WIDE) {
+                        acc += atomicAdd(&win[x], 1u);
+                    } else {
+                        const uint32_t sh = (x & 1u) << 4;
+                        acc += (atomicAdd(&win[x >> 1], 1u << sh) >> sh) & 0xffffu;
+                    }
+                }
+            }
+            __syncthreads();
+        }
     }
     if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
 }
 
 }  // namespace
 
-size_t wedge_arena_bytes(int n_jobs, uint64_t n_total, int workers, uint32_t max_n) {
+size_t wedge_arena_bytes(int n_jobs, uint64_t n_total) {
     return Arena::round(sizeof(WJob) * (size_t)std::max(n_jobs, 1)) +
            Arena::round(sizeof(uint32_t) * 3 * std::max<uint64_t>(n_total, 1)) + Arena::round(sizeof(unsigned int) * 8) +
-           Arena::round(sizeof(unsigned long long) * 4) + Arena::round(sizeof(uint32_t) * (size_t)workers * max_n);
-}
-
-int wedge_workers(uint32_t max_n) {
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // at most two blocks per SM, and at most ~1 GiB of dense counters
-    const uint64_t cap = (1ull << 30) / (4ull * std::max<uint32_t>(max_n, 1));
-    return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)std::max(sms, 1) * 2, cap));
+           Arena::round(sizeof(unsigned long long) * 4);
 }
 
 khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunch *wl, cudaStream_t s) {
@@ -230,23 +272,24 @@ khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunc
         set_error("a wedge launch serves at most 2^32 - 1 start vertices");
         return KHZ_ERR_ARG;
     }
-    for (const auto &j : jobs) L.max_n = std::max(L.max_n, j.n);
-    L.workers = wedge_workers(L.max_n);
+    for (const auto &j : jobs) L.wide = L.wide || j.max_deg >= 65535u;
     WJob *d_jobs = arena->take<WJob>(jobs.size());
     L.lists = arena->take<uint32_t>(3 * std::max<uint64_t>(L.n_total, 1));
     L.cnt = arena->take<unsigned int>(8);
     L.queues = arena->take<unsigned long long>(4);
-    L.dense = arena->take<uint32_t>((size_t)L.workers * std::max<uint32_t>(L.max_n, 1));
-    if (!d_jobs || !L.lists || !L.cnt || !L.queues || !L.dense) {
+    if (!d_jobs || !L.lists || !L.cnt || !L.queues) {
         set_error("wedge launch arena too small");
         return KHZ_ERR_OOM;
     }
     L.list_cap = std::max<uint64_t>(L.n_total, 1);
     if (!jobs.empty())
         KHZ_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(WJob) * jobs.size(), cudaMemcpyHostToDevice, s));
-    KHZ_CUDA(cudaMemsetAsync(L.dense, 0, sizeof(uint32_t) * (size_t)L.workers * std::max<uint32_t>(L.max_n, 1), s));
     KHZ_CUDA(cudaFuncSetAttribute(wedge_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(2 * kBlockSlots * sizeof(uint32_t))));
+    KHZ_CUDA(cudaFuncSetAttribute(wedge_window_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kWinWords * sizeof(uint32_t))));
+    KHZ_CUDA(cudaFuncSetAttribute(wedge_window_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kWinWords * sizeof(uint32_t))));
     int dev = 0;
     KHZ_CUDA(cudaGetDevice(&dev));
     KHZ_CUDA(cudaDeviceGetAttribute(&L.sms, cudaDevAttrMultiProcessorCount, dev));
@@ -264,9 +307,9 @@ khz_status wedge_enqueue(const WedgeLaunch &L, uint64_t *d_rows, cudaStream_t s,
     wedge_warp_kernel<<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.lists, L.cnt + 0, &L.queues[0], d_rows);
     wedge_block_kernel<<<L.sms * 2, kBlockThreads, 2 * kBlockSlots * sizeof(uint32_t), s>>>(
         L.d_jobs, L.n_jobs, L.lists + L.list_cap, L.cnt + 1, &L.queues[1], d_rows);
-    wedge_global_kernel<<<L.workers, kBlockThreads, 0, s>>>(L.d_jobs, L.n_jobs, L.lists + 2 * L.list_cap, L.cnt + 2,
-                                                           &L.queues[2], L.dense, std::max<uint32_t>(L.max_n, 1),
-                                                           d_rows);
+    (L.wide ? wedge_window_kernel<true> : wedge_window_kernel<false>)<<<L.sms, kWinThreads,
+                                                                      kWinWords * sizeof(uint32_t), s>>>(
+        L.d_jobs, L.n_jobs, L.lists + 2 * L.list_cap, L.cnt + 2, &L.queues[2], d_rows);
     KHZ_CUDA(cudaGetLastError());
     if (ls) ls->launches += 4;
     return KHZ_OK;
