@@ -83,16 +83,17 @@ __global__ void wedge_classify_kernel(const WJob *__restrict__ jobs, int n_jobs,
 }
 
 // The part of the sorted list L[0, len) inside [lo, hi), widened to whole gaps between 32 evenly
-// spaced splitters read in one warp-wide load (instead of two binary searches of dependent loads):
-// entries outside [lo, hi) in the returned range are filtered by the caller.
+// spaced splitters (lane l holds splitter l, read in one warp-wide load) instead of two binary
+// searches of dependent loads; entries outside [lo, hi) in the range are filtered by the caller.
 struct Span {
     uint32_t begin, end;
 };
-__device__ __forceinline__ Span splitter_span(const uint32_t *__restrict__ L, uint32_t len, uint32_t lo, uint32_t hi) {
-    const uint32_t lane = lane_id();
+__device__ __forceinline__ uint32_t load_splitter(const uint32_t *__restrict__ L, uint32_t len) {
+    const uint64_t sidx = lane_id() * (((uint64_t)len + 31) >> 5);
+    return sidx < len ? __ldg(L + sidx) : kEmptyKey;
+}
+__device__ __forceinline__ Span splitter_span(uint32_t sp, uint32_t len, uint32_t lo, uint32_t hi) {
     const uint64_t step = ((uint64_t)len + 31) >> 5;
-    const uint64_t sidx = lane * step;
-    const uint32_t sp = sidx < len ? __ldg(L + sidx) : kEmptyKey;
     const uint64_t k_lo = __popc(__ballot_sync(kFull, sp < lo));
     const uint64_t k_hi = __popc(__ballot_sync(kFull, sp < hi));
     Span r;
@@ -101,21 +102,39 @@ __device__ __forceinline__ Span splitter_span(const uint32_t *__restrict__ L, ui
     return r;
 }
 
-// Walk the wedges (v0, w, v2) of one start vertex with the calling threads: warp `wid` of `nw`
-// takes every nw-th w, its lanes take consecutive v2.  f(v2) is called once per wedge.
+// Walk the wedges (v0, w, v2) of one start vertex with w > v0 and v2 in [lo, hi) (lo > v0), with
+// the calling threads: warp `wid` of `nw` takes every nw-th w, its lanes take consecutive v2.  The
+// list bounds of a warp's next 32 w are read together (one per lane), and the next list's
+// splitters are loaded before the current list is walked, so the round trips of one w overlap the
+// previous one's work.  f(v2) is called once per wedge.
 template <typename F>
-__device__ __forceinline__ void walk_wedges(const WJob &J, uint32_t v0, int wid, int nw, F f) {
+__device__ __forceinline__ void walk_wedges(const WJob &J, uint32_t v0, int wid, int nw, uint32_t lo, uint32_t hi,
+                                            F f) {
     const unsigned lane = lane_id();
     const uint64_t b = J.off[v0], e = J.off[v0 + 1];
     const uint32_t start = upper_bound_u32(J.adj + b, 0, (uint32_t)(e - b), v0);
-    for (uint64_t i = b + start + wid; i < e; i += nw) {
-        const uint32_t w = J.adj[i];
-        const uint64_t wb = J.off[w];
-        const uint32_t len = (uint32_t)(J.off[w + 1] - wb);
-        const Span sp = splitter_span(J.adj + wb, len, v0 + 1, kEmptyKey);
-        for (uint64_t k = wb + sp.begin + lane; k < wb + sp.end; k += 32) {
-            const uint32_t v2 = __ldg(J.adj + k);
-            if (v2 > v0) f(v2);
+    for (uint64_t i0 = b + start + wid; i0 < e; i0 += 32ull * nw) {
+        const uint64_t mine = i0 + (uint64_t)lane * nw;
+        uint64_t my_b = 0;
+        uint32_t my_len = 0;
+        if (mine < e) {
+            const uint32_t w = J.adj[mine];
+            my_b = J.off[w];
+            my_len = (uint32_t)(J.off[w + 1] - my_b);
+        }
+        const int nr = (int)min((uint64_t)32, (e - i0 + nw - 1) / nw);
+        uint32_t sp_next = load_splitter(J.adj + __shfl_sync(kFull, my_b, 0), __shfl_sync(kFull, my_len, 0));
+        for (int r = 0; r < nr; ++r) {
+            const uint64_t wb = __shfl_sync(kFull, my_b, r);
+            const uint32_t len = __shfl_sync(kFull, my_len, r);
+            const uint32_t sp = sp_next;
+            if (r + 1 < nr)
+                sp_next = load_splitter(J.adj + __shfl_sync(kFull, my_b, r + 1), __shfl_sync(kFull, my_len, r + 1));
+            const Span s2 = splitter_span(sp, len, lo, hi);
+            for (uint64_t k = wb + s2.begin + lane; k < wb + s2.end; k += 32) {
+                const uint32_t v2 = __ldg(J.adj + k);
+                if (v2 - lo < hi - lo) f(v2);
+            }
         }
     }
 }
@@ -155,7 +174,8 @@ __global__ void __launch_bounds__(256) wedge_warp_kernel(const WJob *__restrict_
             cnts[k] = 0;
         }
         __syncwarp();
-        walk_wedges(jobs[j], (uint32_t)(gv - jobs[j].vbase), 0, 1,
+        const uint32_t v0 = (uint32_t)(gv - jobs[j].vbase);
+        walk_wedges(jobs[j], v0, 0, 1, v0 + 1, jobs[j].n,
                     [&](uint32_t v2) { acc += hash_increment(keys, cnts, kWarpSlots - 1, v2); });
     }
     if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
@@ -190,7 +210,8 @@ __global__ void __launch_bounds__(kBlockThreads) wedge_block_kernel(const WJob *
             cnts[k] = 0;
         }
         __syncthreads();
-        walk_wedges(jobs[j], (uint32_t)(gv - jobs[j].vbase), wid, nw,
+        const uint32_t v0 = (uint32_t)(gv - jobs[j].vbase);
+        walk_wedges(jobs[j], v0, wid, nw, v0 + 1, jobs[j].n,
                     [&](uint32_t v2) { acc += hash_increment(keys, cnts, kBlockSlots - 1, v2); });
         __syncthreads();
     }
@@ -228,28 +249,19 @@ __global__ void __launch_bounds__(kWinThreads, 1) wedge_window_kernel(const WJob
         }
         const WJob &J = jobs[j];
         const uint32_t v0 = (uint32_t)(gv - J.vbase);
-        const uint64_t b = J.off[v0], e = J.off[v0 + 1];
-        const uint32_t start = upper_bound_u32(J.adj + b, 0, (uint32_t)(e - b), v0);
         for (uint64_t base = (uint64_t)v0 + 1; base < J.n; base += span) {
             for (uint32_t t = threadIdx.x; t < kWinWords; t += blockDim.x) win[t] = 0;
             __syncthreads();
-            const uint64_t top = min((uint64_t)J.n, base + span);
-            for (uint64_t i = b + start + wid; i < e; i += nw) {
-                const uint32_t w = J.adj[i];
-                const uint64_t wb = J.off[w];
-                const uint32_t len = (uint32_t)(J.off[w + 1] - wb);
-                const Span sp = splitter_span(J.adj + wb, len, (uint32_t)base, (uint32_t)top);
-                for (uint64_t k = wb + sp.begin + lane; k < wb + sp.end; k += 32) {
-                    const uint32_t x = __ldg(J.adj + k) - (uint32_t)base;
-                    if (x >= (uint32_t)(top - base)) continue;  // outside the window (unsigned)
-                    if (WIDE) {
-                        acc += atomicAdd(&win[x], 1u);
-                    } else {
-                        const uint32_t sh = (x & 1u) << 4;
-                        acc += (atomicAdd(&win[x >> 1], 1u << sh) >> sh) & 0xffffu;
-                    }
+            const uint32_t top = (uint32_t)min((uint64_t)J.n, base + span);
+            walk_wedges(J, v0, wid, nw, (uint32_t)base, top, [&](uint32_t v2) {
+                const uint32_t x = v2 - (uint32_t)base;
+                if (WIDE) {
+                    acc += atomicAdd(&win[x], 1u);
+                } else {
+                    const uint32_t sh = (x & 1u) << 4;
+                    acc += (atomicAdd(&win[x >> 1], 1u << sh) >> sh) & 0xffffu;
                 }
-            }
+            });
             __syncthreads();
         }
     }
