@@ -11,7 +11,8 @@ being the reference engine's own extension counter (engine.cc:924) for that sche
   flush is needed between steps.
 * e2e: the C-ABI path a user takes with host buffers: upload the oriented .dgraph edge list
   from pinned memory, device CSR build, count, copy the result back.
-* roofline: algorithmic bytes of the dominant kernel (instrumented run) / its measured time.
+* roofline: algorithmic bytes of the dominant kernel (instrumented run) / its measured time;
+  traffic = its DRAM bytes per launch from the committed ncu capture (profiles/).
 * cpu_baseline: the reference's own kautomine four_clique app (oracle/_ref, compiled from the
   reference's sources) on a label-restricted slice of the start vertices, all host threads.
 * --impl reference: the same reference binary as the timed arm, on the same slice.
@@ -220,11 +221,15 @@ def ours(args, rank, world, local):
     dom_bytes = st_stats.phase_bytes[dom]
     peak, peak_kind = peaks()
     achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
+    # DRAM bytes per launch of that kernel from the committed ncu capture of this workload
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
+    tpath = os.path.join(ROOT, "profiles", "dram_clique4_rmat22.md")
+    if (args.scale, args.edge_factor) == (SCALE, EDGE_FACTOR) and os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(khz.Stats.PHASES[dom])
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == khz.Stats.PHASES[dom]:
+                    traffic = int(parts[2])
 
     # e2e: oriented .dgraph edge list in pinned host memory -> C ABI -> count -> host
     if args.no_e2e:
