@@ -1489,14 +1489,18 @@ khz_status khz_autotune(khz_ctx *ctx, const khz_job *jobs, int n_jobs, int reps,
     const int warps[] = {8, 16, 32};
     const int chunks[] = {2, 8, 32};
     const int warp_max[] = {32, 64};
+    const int hub_rows[] = {0, -1, 8192};  // auto (32768 on large graphs), none, a small triangle
     for (int pass = 0; pass < 2 && st == KHZ_OK; ++pass) {
-        for (int knob = 0; knob < 4 && st == KHZ_OK; ++knob) {
-            const int *vals = knob == 0 ? engines : knob == 1 ? warps : knob == 2 ? chunks : warp_max;
-            const int nv = knob == 0 ? 2 : knob == 1 ? 3 : knob == 2 ? 3 : 2;
+        for (int knob = 0; knob < 5 && st == KHZ_OK; ++knob) {
+            const int *vals = knob == 0 ? engines : knob == 1 ? warps : knob == 2 ? chunks : knob == 3 ? warp_max : hub_rows;
+            const int nv = knob == 0 ? 2 : knob == 1 ? 3 : knob == 2 ? 3 : knob == 3 ? 2 : 3;
             for (int v = 0; v < nv && st == KHZ_OK; ++v) {
                 khz_config c = best;
-                int *field = knob == 0 ? &c.engine : knob == 1 ? &c.dfs_warps_per_sm : knob == 2 ? &c.dfs_chunk
-                                                                                                 : &c.bitmap_warp_max;
+                int *field = knob == 0   ? &c.engine
+                             : knob == 1 ? &c.dfs_warps_per_sm
+                             : knob == 2 ? &c.dfs_chunk
+                             : knob == 3 ? &c.bitmap_warp_max
+                                         : &c.bitmap_hub_rows;
                 if (*field == vals[v]) continue;
                 *field = vals[v];
                 double ms = 0;

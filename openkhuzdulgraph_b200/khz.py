@@ -293,7 +293,7 @@ class Context:
         b = rep.best
         return {"trials": rep.trials, "baseline_ms": rep.baseline_ms, "best_ms": rep.best_ms,
                 "engine": b.engine, "dfs_warps_per_sm": b.dfs_warps_per_sm, "dfs_chunk": b.dfs_chunk,
-                "bitmap_warp_max": b.bitmap_warp_max}
+                "bitmap_warp_max": b.bitmap_warp_max, "bitmap_hub_rows": b.bitmap_hub_rows}
 
     def count_batch(self, jobs, stream=None):
         """jobs: list of (Graph, app) -> (list of count lists, list of NumExtensions, Stats)"""
