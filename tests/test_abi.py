@@ -50,3 +50,10 @@ def test_errors_are_codes_not_aborts():
     L = khz.lib()
     assert L.khz_set_op_batch(42, None, None, None, None, None, None, None, 0, None) == 1
     assert L.khz_ctx_set_config(None, None) == 1
+
+
+def test_config_layout_is_fixed():
+    """khz_config keeps its size when fields are taken from the reserved words (64 bytes)."""
+    import ctypes
+    assert ctypes.sizeof(khz.Config) == 64
+    assert khz.Config.bitmap_hub_rows.offset == 24 and khz.Config.reserved.offset == 28
