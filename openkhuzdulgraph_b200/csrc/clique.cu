@@ -15,11 +15,13 @@
 // also sums the schedule's algorithmic bytes 4 * (|A| + |B| + |A n B|) per set op.
 //
 // One launch sequence serves many (graph, clique app) jobs: their start vertices form one
-// global index space.  Tiers by out-degree d of v0: one warp per v0 for d <= 64 (rows of 2
-// words), one block per v0 for 64 < d <= 256 and 256 < d <= kBlockMax (rows in up to ~219 KB
-// of shared memory, sized from the largest out-degree of the batch); larger d are left to the
-// DFS engine.  Device-side classification sorts the block-tier start vertices into degree
-// buckets, heaviest bucket first, so nothing waits on the host between launches.
+// global index space.  Tiers by out-degree d of v0: one warp per v0 for d <= 64, one block per
+// v0 for 64 < d <= 256 and 256 < d <= kBlockMax (rows in up to ~227 KB of shared memory, sized
+// from the largest out-degree of the batch); larger d are left to the DFS engine.  Device-side
+// classification sorts the block-tier start vertices by degree, heaviest first, so nothing
+// waits on the host between launches.  Rows of the highest-ranked vertices come from a
+// per-job hub triangle (one bit test per candidate pair); the others from splitter-bounded
+// scans of the candidate's out-list against a hash of C.
 #include <cuda_runtime.h>
 
 #include "khz_internal.cuh"
