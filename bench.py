@@ -106,16 +106,20 @@ class ClockSampler:
 
 
 def dist_setup(gpus):
+    """One process per GPU (torchrun env).  The process group is NCCL; KHZ_BENCH_DIST_BACKEND=gloo
+    selects gloo for CPU-only runs of the rank plumbing."""
     rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(os.environ.get("KHZ_BENCH_DIST_BACKEND", "nccl"),
+                                timeout=datetime.timedelta(seconds=300))
     return rank, world, local
 
 
 def max_over_ranks(x, world, device):
+    """The maximum of x over all ranks (device: the local CUDA device index, or "cpu")."""
     if world == 1:
         return x
     import torch
@@ -126,11 +130,16 @@ def max_over_ranks(x, world, device):
 
 
 def barrier(world, device):
+    """All ranks meet, then the local device drains (device: CUDA index, or "cpu")."""
     import torch
     if world > 1:
         import torch.distributed as dist
-        dist.barrier(device_ids=[device])
-    torch.cuda.synchronize()
+        if isinstance(device, int):
+            dist.barrier(device_ids=[device])
+        else:
+            dist.barrier()
+    if isinstance(device, int):
+        torch.cuda.synchronize()
 
 
 # ------------------------------------------------------------------------------ reference / CPU

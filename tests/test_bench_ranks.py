@@ -1,0 +1,56 @@
+"""The bench's multi-rank plumbing (one process per GPU under torchrun) on CPU: two gloo ranks
+rendezvous through the same helpers, agree on the maximum of their timings and meet at barriers."""
+import os
+import socket
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, out):
+    os.environ.update({"RANK": str(rank), "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank),
+                       "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port),
+                       "KHZ_BENCH_DIST_BACKEND": "gloo"})
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    import bench
+    r, w, local = bench.dist_setup(world)
+    assert (r, w, local) == (rank, world, rank)
+    bench.barrier(w, "cpu")
+    m = bench.max_over_ranks(10.0 * (rank + 1) + 0.5, w, "cpu")
+    bench.barrier(w, "cpu")
+    out.put((rank, m))
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_agree_on_max():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    codes = [p.exitcode for p in procs]
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert codes == [0, 0]
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    assert got == [(0, 20.5), (1, 20.5)]
+
+
+def test_single_rank_needs_no_process_group():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.max_over_ranks(3.25, 1, "cpu") == 3.25
