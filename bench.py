@@ -232,7 +232,7 @@ def ours(args, rank, world, local):
     achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
     # DRAM bytes per launch of that kernel from the committed ncu capture of this workload
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "dram_clique4_rmat22.md")
+    tpath = os.path.join(ROOT, "profiles", "dram_clique4_rmat22.txt")
     if (args.scale, args.edge_factor) == (SCALE, EDGE_FACTOR) and os.path.exists(tpath):
         with open(tpath) as f:
             for line in f:
