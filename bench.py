@@ -105,6 +105,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def profile_traffic(kernel):
+    """DRAM bytes (read + write) per launch of a bench kernel, from the committed ncu summary of the
+    bench workload (lines `traffic_bytes_per_launch <kernel> <bytes>`), or None."""
+    path = os.path.join(ROOT, "profiles", "dram_clique4_rmat22.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                return int(parts[2])
+    return None
+
+
 def dist_setup(gpus):
     """One process per GPU (torchrun env).  The process group is NCCL; KHZ_BENCH_DIST_BACKEND=gloo
     selects gloo for CPU-only runs of the rank plumbing."""
@@ -232,13 +246,8 @@ def ours(args, rank, world, local):
     achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
     # DRAM bytes per launch of that kernel from the committed ncu capture of this workload
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "dram_clique4_rmat22.txt")
-    if (args.scale, args.edge_factor) == (SCALE, EDGE_FACTOR) and os.path.exists(tpath):
-        with open(tpath) as f:
-            for line in f:
-                parts = line.split()
-                if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == khz.Stats.PHASES[dom]:
-                    traffic = int(parts[2])
+    if (args.scale, args.edge_factor) == (SCALE, EDGE_FACTOR):
+        traffic = profile_traffic(khz.Stats.PHASES[dom])
 
     # e2e: oriented .dgraph edge list in pinned host memory -> C ABI -> count -> host
     if args.no_e2e:

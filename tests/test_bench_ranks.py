@@ -54,3 +54,12 @@ def test_single_rank_needs_no_process_group():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.max_over_ranks(3.25, 1, "cpu") == 3.25
+
+
+def test_bench_reads_kernel_traffic_from_the_profile():
+    sys.path.insert(0, ROOT)
+    import bench
+    from openkhuzdulgraph_b200 import khz
+    got = {k: bench.profile_traffic(k) for k in khz.Stats.PHASES[:3]}
+    assert all(isinstance(v, int) and v > 0 for v in got.values()), got
+    assert bench.profile_traffic("no_such_kernel") is None
