@@ -119,6 +119,47 @@ def profile_traffic(kernel):
     return None
 
 
+def profile_counters(kernel):
+    """Issue-active fraction, IPC and L2 hit rate of a bench kernel from the committed ncu capture of
+    its small case (lines `ncu_counter <kernel> <name> <value>`), as a dict (empty if absent)."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "clique_block_kernel_rmat21.md")
+    if not os.path.exists(path):
+        return out
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) == 4 and parts[0] == "ncu_counter" and parts[1] == kernel:
+                out[parts[2]] = float(parts[3])
+    return out
+
+
+def host_cpu():
+    """CPU model, physical cores and logical CPUs of this host."""
+    model, cores = "unknown", set()
+    phys = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name":
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None and core is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+        if phys is not None and core is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    logical = os.cpu_count() or 1
+    return model, (len(cores) or logical), logical
+
+
 def dist_setup(gpus):
     """One process per GPU (torchrun env).  The process group is NCCL; KHZ_BENCH_DIST_BACKEND=gloo
     selects gloo for CPU-only runs of the rank plumbing."""
@@ -169,24 +210,60 @@ def labelled_oriented_dgraph(g, tmpdir):
 
 def run_reference_sample(dgraph, runs):
     """The reference's own kautomine four_clique (apply + engine, compiled unmodified) over the
-    start vertices of label class 0; returns (per-run seconds, embeddings per run, kind, cores)."""
+    start vertices of label class 0.  Returns a dict: per-run seconds, embeddings, count and
+    NumExtensions per run, kind ("reference" or "port"), threads used."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
-    cores = os.cpu_count() or 1
+    logical = os.cpu_count() or 1
     exe = os.path.join(orc.REF_DIR, "sample_" + APP)
     if os.path.exists(exe):
         counts, avg_ms, ext = orc.run_reference(APP, dgraph, threads=-1, runs=runs, label=0, timeout=3000)
         per_run_ext = ext // runs
-        threads = max(1, cores - 2)  # the reference caps compute threads at cores - 2 (distributed_application.cc:80)
-        return avg_ms / 1000.0, per_run_ext + counts[0], "reference", threads
+        threads = max(1, logical - 2)  # the reference caps compute threads at CPUs - 2 (distributed_application.cc:80)
+        return {"secs": avg_ms / 1000.0, "embeddings": per_run_ext + counts[0], "count": counts[0],
+                "num_extensions": per_run_ext, "kind": "reference", "threads": threads}
     # the oracle port (C restatement) when the reference binaries are not present
     n, pairs, _ = orc.read_dgraph(dgraph)
     off, adj = orc.csr(pairs, n)
     t0 = time.time()
     for _ in range(runs):
-        counts, ext, _ = orc.count(APP, off, adj, v0_mod=SAMPLE_MOD, v0_rem=0, threads=cores)
+        counts, ext, _ = orc.count(APP, off, adj, v0_mod=SAMPLE_MOD, v0_rem=0, threads=logical)
     dt = (time.time() - t0) / runs
-    return dt, ext + counts[0], "port", cores
+    return {"secs": dt, "embeddings": ext + counts[0], "count": counts[0], "num_extensions": ext, "kind": "port",
+            "threads": logical}
+
+
+def reference_built_graph(scale, edge_factor, tmpdir):
+    """The bench graph made without this repository's library: the oracle's generator (bit-identical
+    to the device generator) writes the edge list, the reference's own converter and
+    to_oriented_dataset_converter build the oriented .dgraph, and the node labels v % SAMPLE_MOD are
+    inserted after its header.  Returns the labelled file's path (or None without oracle/_ref)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    conv = os.path.join(orc.REF_DIR, "converter")
+    ori = os.path.join(orc.REF_DIR, "to_oriented_dataset_converter")
+    if not (os.path.exists(conv) and os.path.exists(ori)):
+        return None
+    a, b, c = RMAT_ABC
+    canon, n = orc.rmat(scale, edge_factor, a, b, c, seed=SEED)
+    base = os.path.join(tmpdir, "k")
+    canon.astype(np.uint32).tofile(base + ".biedgelist")
+    del canon
+    subprocess.run([conv, base, base, str(n), "0", "0", "0"], check=True, stdout=subprocess.DEVNULL)
+    os.remove(base + ".biedgelist")
+    subprocess.run([ori, base + ".dgraph", base + ".oriented"], check=True, stdout=subprocess.DEVNULL)
+    os.remove(base + ".dgraph")
+    raw = np.fromfile(base + ".oriented", dtype=np.uint8)
+    os.remove(base + ".oriented")
+    hdr = raw[:20].copy()
+    hdr[12:16] = np.frombuffer(np.int32(1).tobytes(), dtype=np.uint8)  # has_node_label
+    path = os.path.join(tmpdir, "k_oriented_labeled.dgraph")
+    with open(path, "wb") as f:
+        f.write(hdr.tobytes())
+        f.write((np.arange(n, dtype=np.uint64) % SAMPLE_MOD).astype(np.uint32).tobytes())
+        f.write(raw[20:].tobytes())
+    return path
 
 
 # ------------------------------------------------------------------------------ main arms
@@ -238,16 +315,20 @@ def ours(args, rank, world, local):
     ms_per_step = total_ms / args.steps
     value = embeddings * world / (ms_per_step / 1000.0)
 
-    # dominant kernel and its roofline
+    # dominant kernel and its roofline: DRAM bytes it moves per launch (committed ncu capture of this
+    # workload) over its CUDA-event time, against the measured HBM copy bandwidth; the reference
+    # schedule's algorithmic bytes over the same time are reported beside it (algo_gbs), since the
+    # bitmap engine replaces list intersections by bit-matrix popcounts and never moves those bytes
     dom = max(range(4), key=lambda p: phase_ms[p])
     dom_ms = phase_ms[dom] / args.steps
     dom_bytes = st_stats.phase_bytes[dom]
     peak, peak_kind = peaks()
-    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
-    # DRAM bytes per launch of that kernel from the committed ncu capture of this workload
+    algo_gbs = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else 0.0
     traffic = None
     if (args.scale, args.edge_factor) == (SCALE, EDGE_FACTOR):
         traffic = profile_traffic(khz.Stats.PHASES[dom])
+    dram_gbs = traffic / (dom_ms / 1000.0) / 1e9 if traffic and dom_ms > 0 else None
+    counters = profile_counters(khz.Stats.PHASES[dom])
 
     # e2e: oriented .dgraph edge list in pinned host memory -> C ABI -> count -> host
     if args.no_e2e:
@@ -285,12 +366,22 @@ def ours(args, rank, world, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        import numpy as np
         with tempfile.TemporaryDirectory() as td:
             path = labelled_oriented_dgraph(g, td)
-            secs, emb, kind, cores = run_reference_sample(path, runs=1)
-        cpu = {"value": emb / secs, "unit": "embeddings/s", "cores": cores, "kind": kind,
-               "sample": "start vertices v0 %% %d == 0 of the same oriented graph (%d embeddings, %.1f s)"
-                         % (SAMPLE_MOD, emb, secs)}
+            r = run_reference_sample(path, runs=1)
+        # the same slice on the device (restrict_starting_vertex_label): the reference's count and
+        # NumExtensions must be the device's
+        g.set_labels((np.arange(n, dtype=np.uint64) % SAMPLE_MOD).astype(np.uint32))
+        slice_counts, slice_st = ctx.count_restricted(g, APP, 0)
+        assert slice_counts[0] == r["count"] and slice_st.num_extensions == r["num_extensions"], \
+            (slice_counts, slice_st.num_extensions, r)
+        model, cores, logical = host_cpu()
+        cpu = {"value": r["embeddings"] / r["secs"], "unit": "embeddings/s", "cores": cores, "threads": r["threads"],
+               "logical_cpus": logical, "cpu_model": model, "kind": r["kind"],
+               "sample": "start vertices v0 %% %d == 0 of the same oriented graph (%d embeddings, %.1f s); "
+                         "count %d and NumExtensions %d equal the device's restricted count of that slice"
+                         % (SAMPLE_MOD, r["embeddings"], r["secs"], r["count"], r["num_extensions"])}
 
     if rank == 0:
         line = {
@@ -305,10 +396,13 @@ def ours(args, rank, world, local):
             "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": int(pairs.numel() * 4),
                     "d2h_bytes_per_step": 8 * 8, "ms_per_step": e2e_total / args.steps,
                     "ms_build_count_free": e2e_parts},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+            "roofline": {"bound": "issue" if dom < 3 else "latency", "achieved": dram_gbs, "peak": peak,
+                         "unit": "GB/s", "frac": dram_gbs / peak if dram_gbs is not None else None,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "basis": "DRAM bytes per launch (ncu, committed capture) / CUDA-event time",
                          "kernel": khz.Stats.PHASES[dom], "kernel_ms": dom_ms,
-                         "algo_bytes_per_launch": dom_bytes},
+                         "algo_bytes_per_launch": dom_bytes, "algo_gbs": algo_gbs, "algo_frac": algo_gbs / peak,
+                         "ncu_small_case": counters},
             "phase_ms_per_step": [x / args.steps for x in phase_ms],
             "phase_algo_bytes": list(st_stats.phase_bytes),
             "gpu_launches": launches,
@@ -511,27 +605,41 @@ def serve_workload(args):
 
 
 def reference_arm(args, rank, world, local):
+    """The reference's own CPU path only: the graph is built by the oracle generator and the
+    reference's converters (reference_built_graph), and the reference's kautomine four_clique
+    counts the label-0 slice of its start vertices; this repository's library is not loaded."""
     if rank != 0:
         return
-    from openkhuzdulgraph_b200 import khz
-    import torch
-    torch.cuda.set_device(local)
-    ctx = khz.Context(local)
-    a, b, c = RMAT_ABC
-    sym = ctx.generate_rmat(args.scale, args.edge_factor, a, b, c, SEED)
-    g = sym.orient()
-    sym.free()
+    import numpy as np
+    t0 = time.time()
     with tempfile.TemporaryDirectory() as td:
-        path = labelled_oriented_dgraph(g, td)
-        ctx.close()
-        secs, emb, kind, cores = run_reference_sample(path, runs=args.steps)
-    value = emb / secs
+        path = reference_built_graph(args.scale, args.edge_factor, td)
+        if path is None:  # no oracle/_ref: the oracle restatement of the same schedule
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import orc
+            a, b, c = RMAT_ABC
+            canon, n = orc.rmat(args.scale, args.edge_factor, a, b, c, seed=SEED)
+            off, adj = orc.csr(orc.symmetrize(canon), n)
+            ooff, oadj, _ = orc.orient(off, adj)
+            src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(ooff).astype(np.int64))
+            path = os.path.join(td, "k_oriented_labeled.dgraph")
+            orc.write_dgraph(path, n, np.stack([src, oadj], axis=1),
+                             (np.arange(n, dtype=np.uint64) % SAMPLE_MOD).astype(np.uint32))
+        t_build = time.time() - t0
+        r = run_reference_sample(path, runs=args.steps)
+    value = r["embeddings"] / r["secs"]
+    model, cores, logical = host_cpu()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "embeddings/s", "n_gpus": 0,
-            "steps": args.steps, "warmup": 0, "ms_per_step": secs * 1000.0, "higher_is_better": True,
+            "steps": args.steps, "warmup": 0, "ms_per_step": r["secs"] * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": "v0 %% %d == 0" % SAMPLE_MOD},
-            "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": cores, "kind": kind,
-                             "sample": "start vertices v0 %% %d == 0 (%d embeddings per step)" % (SAMPLE_MOD, emb)},
+            "config": {"workload": WORKLOAD, "sample": "v0 %% %d == 0" % SAMPLE_MOD, "same_config": False,
+                       "graph_built_by": "oracle generator + reference converter + to_oriented_dataset_converter",
+                       "graph_build_s": t_build},
+            "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": cores, "threads": r["threads"],
+                             "logical_cpus": logical, "cpu_model": model, "kind": r["kind"],
+                             "sample": "start vertices v0 %% %d == 0 (%d embeddings per step; count %d, "
+                                       "NumExtensions %d)" % (SAMPLE_MOD, r["embeddings"], r["count"],
+                                                              r["num_extensions"])},
             "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define KHZ_ABI_VERSION 1
+#define KHZ_ABI_VERSION 2
 
 /* Error codes.  Replaces the reference's assert()/exit(-1) failure paths
  * (e.g. distributed_application.cc:281-282, engine.cc:53-55, kautomine/triangle.cc:112-119). */
@@ -65,6 +65,8 @@ typedef uint32_t khz_graph; /* 0 is never a valid handle */
 #define KHZ_EDGES_ON_DEVICE 0x1u /* the pairs pointer is device memory */
 #define KHZ_ORIENT 0x2u          /* store the degree-oriented DAG instead of the symmetric CSR */
 #define KHZ_UNCHECKED 0x4u       /* skip the sortedness/range validation pass */
+#define KHZ_SKIP_LABELS 0x8u     /* khz_graph_load_dgraph: do not keep the file's node labels
+                                    (DistributedApplication's load_vertex_labels = false) */
 
 /* engine choice (khz_config.engine) */
 #define KHZ_ENGINE_AUTO 0
@@ -79,8 +81,11 @@ typedef struct khz_graph_info {
     int32_t oriented;      /* 1: every list holds only larger ids (a DAG in id order) */
     int32_t symmetric;     /* 1: every entry has its reverse (undirected form) */
     const uint64_t *d_offsets; /* device, num_vertices + 1 */
-    const uint32_t *d_adj;     /* device, num_entries (+ 4 padding entries) */
+    const uint32_t *d_adj;     /* device, num_entries (+ 8 padding entries) */
     uint64_t device_bytes;     /* HBM held by this graph */
+    uint32_t num_labels;       /* 0: no node labels */
+    uint32_t reserved;
+    const uint32_t *d_labels;  /* device, num_vertices, or NULL */
 } khz_graph_info;
 
 typedef struct khz_stats {
@@ -142,6 +147,12 @@ khz_status khz_graph_info_get(khz_ctx *ctx, khz_graph g, khz_graph_info *info);
 khz_status khz_graph_export_csr(khz_ctx *ctx, khz_graph g, uint64_t *offsets, uint32_t *adj);
 /* Writes the graph as a .dgraph file (symmetric or oriented, as stored); labels may be NULL. */
 khz_status khz_graph_write_dgraph(khz_ctx *ctx, khz_graph g, const char *path, const uint32_t *labels);
+/* Attaches node labels (labels: host array of num_vertices uint32) to a graph, replacing any it
+ * had.  Labels must be dense: every value in [0, max label] is used by some vertex, as the
+ * reference's loader requires (graph_loader.h:795-804, which exits otherwise; here KHZ_ERR_FORMAT).
+ * khz_graph_load_dgraph attaches a labelled file's labels itself (graph_loader.h:773-822).
+ * Orientation relabels vertices and, like to_oriented_dataset_converter.cc:76, drops labels. */
+khz_status khz_graph_set_labels(khz_ctx *ctx, khz_graph g, const uint32_t *labels, uint32_t num_vertices);
 /* Frees the graph's HBM.  Replaces destroy_graphs (graph_loader.h:963-974). */
 khz_status khz_graph_free(khz_ctx *ctx, khz_graph g);
 
@@ -155,6 +166,17 @@ khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts
 /* Enqueues the same work without waiting: d_out (device, >= 8 uint64) receives
  * [0..5] counts, [6] NumExtensions, [7] algorithmic bytes (0 unless configured). */
 khz_status khz_count_async(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *d_out, void *stream);
+/* run(disable_output, restrict_starting_vertex_label = true, start_label): the same count with the
+ * start vertices v_0 restricted to the vertices whose label is start_label
+ * (distributed_application.h:54, WorkloadDistributer::fetch_next_batch_local, engine.cc:1457-1496).
+ * The graph must carry labels.  counts receives the aggregators' RAW values (Aggregator::evaluate,
+ * engine.h:630-645): on a slice of the start vertices a pattern's copies need not come in whole
+ * multiples of its multiplicity, so the division is left to the caller, as the reference apps do
+ * after run().  stats->num_extensions is the restricted run's NumExtensions.  Clique apps use the
+ * bitmap engine only on a graph stored oriented (its start vertices are the stored ones); on other
+ * graphs the schedule runs as stored on the DFS engine. */
+khz_status khz_count_restricted(khz_ctx *ctx, khz_graph g, khz_app_id app, uint32_t start_label, uint64_t *counts,
+                                khz_stats *stats, void *stream);
 int khz_app_num_counts(khz_app_id app);
 /* mirrors the reference's `multiplicities[]` tables (kautomine/three_motif.cc:44) */
 int khz_app_multiplicity(khz_app_id app, int pattern);
@@ -251,12 +273,14 @@ khz_status khz_set_op_batch(int op, const uint64_t *a_off, const uint32_t *a, co
  * CSR (d_offsets: n + 1 uint64, d_adj: num_entries uint32) with the DFS engine and writes the
  * same 8 uint64 as khz_count_async to the caller's device buffer d_out: [0..5] counts,
  * [6] NumExtensions, [7] 0.  It allocates nothing: all scratch lives in one fixed device array
- * of about 14.6 MiB inside the library, which every GPU that loads the library holds until the
- * process exits.  Limits: graphs whose largest vertex degree is at most 1024 (larger ones get
- * KHZ_ERR_ARG).  The first call on each device looks up the array's device address with that
- * device current, so make that first call before any stream capture.  Every call shares the
- * array: calls whose work overlaps on the GPU (other streams, other host threads) race and must
- * be serialised by the caller.  Returns once d_out holds the result. */
+ * of 14,557,184 bytes (about 13.9 MiB) inside the library, which every GPU that loads the library
+ * holds until the process exits.  Limits: graphs whose largest vertex degree is at most 1024
+ * (larger ones get KHZ_ERR_ARG).  The first call on each device looks up the array's device
+ * address with that device current, so make that first call before any stream capture.  Every
+ * call shares the array: calls whose work overlaps on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller.  Each call waits on its stream twice (to read the
+ * graph's largest degree before the launch and the divisibility flag after it) and returns once
+ * d_out holds the result. */
 khz_status khz_count_noalloc(const uint64_t *d_offsets, const uint32_t *d_adj, uint32_t n, uint64_t num_entries,
                              khz_app_id app, uint64_t *d_out, void *stream);
 

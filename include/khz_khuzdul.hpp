@@ -52,9 +52,11 @@ class DistributedApplication {
     DistributedApplication(int num_threads, const std::string &graph_path, int max_pattern_size,
                            khz_app_id schedule, bool load_vertex_labels = false, int device = 0)
         : num_threads_(num_threads), max_pattern_size_(max_pattern_size), schedule_(schedule) {
-        (void)load_vertex_labels;
         check(khz_ctx_create(device, &ctx_));
-        khz_status s = khz_graph_load_dgraph(ctx_, graph_path.c_str(), 0, &graph_);
+        // node labels are kept only when asked for, as the reference's loader does
+        // (graph_loader.h:773-822)
+        khz_status s = khz_graph_load_dgraph(ctx_, graph_path.c_str(), load_vertex_labels ? 0u : KHZ_SKIP_LABELS,
+                                             &graph_);
         if (s != KHZ_OK) {
             khz_ctx_destroy(ctx_);
             check(s);
@@ -77,21 +79,24 @@ class DistributedApplication {
     }
 
     // run() (distributed_application.cc:259-356): one count of every pattern of the schedule.
-    // Each aggregator receives its pattern's raw count (multiplied back by the multiplicity, so
-    // the app's own `evaluate() / multiplicities[i]` stays as written).
+    // Each aggregator receives its pattern's raw count (the app's own `evaluate() /
+    // multiplicities[i]` stays as written).  With restrict_starting_vertex_label only the start
+    // vertices of that label are extended (engine.cc:1457-1496); the graph must have been loaded
+    // with load_vertex_labels.
     void run(bool disable_output = false, bool restrict_starting_vertex_label = false, LabelId label = 0) {
         (void)disable_output;
-        if (restrict_starting_vertex_label) {
-            (void)label;
-            throw Error(KHZ_ERR_ARG, "restrict_starting_vertex_label is not supported by the device engine");
-        }
         uint64_t counts[KHZ_MAX_COUNTS];
         khz_stats st;
-        check(khz_count(ctx_, graph_, schedule_, counts, &st, nullptr));
-        num_extensions_ += st.num_extensions;
         const int nc = khz_app_num_counts(schedule_);
+        if (restrict_starting_vertex_label) {
+            check(khz_count_restricted(ctx_, graph_, schedule_, label, counts, &st, nullptr));  // raw counts
+        } else {
+            check(khz_count(ctx_, graph_, schedule_, counts, &st, nullptr));
+            for (int i = 0; i < nc; ++i) counts[i] *= (uint64_t)khz_app_multiplicity(schedule_, i);
+        }
+        num_extensions_ += st.num_extensions;
         for (int i = 0; i < nc && i < (int)aggregators_.size(); ++i)
-            if (aggregators_[i]) aggregators_[i]->set(counts[i] * (uint64_t)khz_app_multiplicity(schedule_, i));
+            if (aggregators_[i]) aggregators_[i]->set(counts[i]);
         last_counts_.assign(counts, counts + nc);
     }
 

@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restr
             const uint64_t gv = n_total - 1 - myc;
             myj = job_of(jobs, n_jobs, gv);
             myv = (uint32_t)(gv - jobs[myj].vbase);
-            myd = odeg(jobs[myj].off, myv);
+            myd = jobs[myj].start.keep(myv) ? odeg(jobs[myj].off, myv) : 0u;
         }
         unsigned todo = __ballot_sync(kFull, myc < c1 && myd >= dmin && myd <= warp_max);
         while (todo) {
@@ -696,7 +696,8 @@ __global__ void classify_count_kernel(const BJob *__restrict__ jobs, int n_jobs,
         uint32_t d = 0;
         if (gv < n_total) {
             j = job_of(jobs, n_jobs, gv);
-            d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
+            const uint32_t v = (uint32_t)(gv - jobs[j].vbase);
+            d = jobs[j].start.keep(v) ? odeg(jobs[j].off, v) : 0u;  // a filtered-out start vertex extends nothing
             if (d > warp_max && d <= (uint32_t)kBlockMax) atomicAdd(&cnt[d], 1u);
         }
         // one atomic per distinct job per warp
@@ -735,7 +736,9 @@ __global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs,
     for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < n_total;
          gv += (uint64_t)gridDim.x * blockDim.x) {
         const int j = job_of(jobs, n_jobs, gv);
-        const uint32_t d = odeg(jobs[j].off, (uint32_t)(gv - jobs[j].vbase));
+        const uint32_t v = (uint32_t)(gv - jobs[j].vbase);
+        if (!jobs[j].start.keep(v)) continue;
+        const uint32_t d = odeg(jobs[j].off, v);
         if (d <= warp_max || d > (uint32_t)kBlockMax) continue;
         const unsigned int pos = cnt[kCntBase + d] + atomicAdd(&cnt[kCntCursor + d], 1u);
         if (d <= (uint32_t)kMidMax) mid_list[pos] = (uint32_t)gv;

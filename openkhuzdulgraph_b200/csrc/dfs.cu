@@ -272,7 +272,12 @@ __global__ void __launch_bounds__(256) dfs_kernel(const DfsJob *__restrict__ job
                 v0 = lo;
                 v0_end = c.off[v0 + 1];
             }
-            if (v0_end - c.off[v0] < J.min_deg) continue;
+            if (v0_end - c.off[v0] < J.min_deg || !J.start.keep(v0)) {
+                // no unit of this start vertex is extended: skip to its last unit in the chunk
+                const uint64_t next = J.unit_begin + v0_end;
+                u = (next < u1 ? next : u1) - 1;
+                continue;
+            }
             const Plan &p = *c.plan;
             const Level &l1 = p.lv[1];
             c.v[0] = v0;

@@ -224,8 +224,12 @@ struct DevBuf {
 void free_graph_memory(Graph *g) {
     dev_free(g->off);
     dev_free(g->adj);
+    dev_free(g->labels);
     g->off = nullptr;
     g->adj = nullptr;
+    g->labels = nullptr;
+    g->num_labels = 0;
+    g->label_count.clear();
 }
 
 khz_status build_csr_from_device_pairs(const uint32_t *d_pairs, uint64_t m, uint32_t n, bool validate, Graph *g,

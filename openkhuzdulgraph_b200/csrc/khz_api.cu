@@ -306,15 +306,19 @@ khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
 // graphs that are a DAG in id order or symmetric (oriented once, cached); the DFS engine otherwise
 // and the wedge engine for the 4-cycle app on symmetric graphs.  Instrumented runs
 // (want_algo_bytes) of the 4-cycle use the DFS engine, which sums the schedule's set-op bytes.
-int pick_engine(const khz_config &cfg, const AppDef &def, int app, const Graph &g) {
+// A start-vertex restriction keeps the start vertices of the graph as stored, so the bitmap engine
+// (which starts from the oriented view's vertices) serves restricted clique jobs only on graphs
+// stored oriented, and the 3-motif identity path (global degree sums) not at all.
+int pick_engine(const khz_config &cfg, const AppDef &def, int app, const Graph &g, bool restricted = false) {
     const bool wedge_ok = app == KHZ_KGPI_4CYCLE && g.symmetric && !cfg.want_algo_bytes;
-    const bool motif3 = (app == KHZ_KAUTO_3MOTIF || app == KHZ_KGPI_3MOTIF) && g.symmetric && !cfg.want_algo_bytes;
+    const bool motif3 = (app == KHZ_KAUTO_3MOTIF || app == KHZ_KGPI_3MOTIF) && g.symmetric && !cfg.want_algo_bytes &&
+                        !restricted;
     int engine = cfg.engine;
     if (engine == KHZ_ENGINE_AUTO)
         engine = def.clique || motif3 ? KHZ_ENGINE_BITMAP : (wedge_ok ? KHZ_ENGINE_WEDGE : KHZ_ENGINE_DFS);
     if (engine == KHZ_ENGINE_BITMAP && motif3) return KHZ_ENGINE_BITMAP;
     if (engine == KHZ_ENGINE_BITMAP && !def.clique) engine = KHZ_ENGINE_DFS;
-    if (engine == KHZ_ENGINE_BITMAP && !g.oriented && !g.symmetric) engine = KHZ_ENGINE_DFS;
+    if (engine == KHZ_ENGINE_BITMAP && !g.oriented && (!g.symmetric || restricted)) engine = KHZ_ENGINE_DFS;
     if (engine == KHZ_ENGINE_WEDGE && !wedge_ok) engine = KHZ_ENGINE_DFS;
     return engine;
 }
@@ -325,8 +329,10 @@ constexpr unsigned kPlanPinned = 2u;     // the plan owns a pinned result buffer
 constexpr unsigned kPlanPoolMem = 4u;    // device scratch from the context's stream-ordered pool on `s`
 constexpr unsigned kPlanFreeLegacy = 8u; // with kPlanPoolMem: release on the legacy stream (callers sync first)
 
+// start_labels (may be null): per job, the label its start vertices are restricted to, or -1.
+// Restricted jobs report raw counts (multiplicities not divided).
 khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, unsigned opts,
-                      std::unique_ptr<BatchPlan> *out) {
+                      std::unique_ptr<BatchPlan> *out, const int64_t *start_labels = nullptr) {
     const bool own_scratch = (opts & kPlanOwnSlots) != 0;
     if (n <= 0) {
         set_error("empty batch");
@@ -337,7 +343,17 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             set_error("invalid app id %d", jobs[i].app);
             return KHZ_ERR_ARG;
         }
-        if (!get_graph(ctx, jobs[i].graph)) return KHZ_ERR_ARG;
+        const Graph *g = get_graph(ctx, jobs[i].graph);
+        if (!g) return KHZ_ERR_ARG;
+        const int64_t lab = start_labels ? start_labels[i] : -1;
+        if (lab >= 0 && !g->labels) {
+            set_error("graph %u has no node labels to restrict the start vertices by", jobs[i].graph);
+            return KHZ_ERR_ARG;
+        }
+        if (lab >= (int64_t)g->num_labels) {
+            set_error("start label %lld out of range: the graph has %u labels", (long long)lab, g->num_labels);
+            return KHZ_ERR_ARG;
+        }
     }
     auto P = std::make_unique<BatchPlan>();
     P->rows = n;
@@ -352,7 +368,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     std::vector<uint32_t> mult((size_t)n * KHZ_MAX_COUNTS, 1);
     uint32_t bmax = 0, slot_cap = 32;
     uint64_t vbase = 0, bm_entries = 0, unit_base = 0, wbase = 0;
-    auto add_dfs = [&](const Graph &g, const Plan &pl, int row, uint32_t min_deg) {
+    auto add_dfs = [&](const Graph &g, const Plan &pl, int row, uint32_t min_deg, StartFilter sf) {
         DfsJob j{};
         j.off = g.off;
         j.adj = g.adj;
@@ -362,6 +378,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         j.num_units = g.m;
         j.out_base = (uint32_t)row;
         j.min_deg = min_deg;
+        j.start = sf;
         plans.push_back(pl);
         djobs.push_back(j);
         unit_base += g.m;
@@ -371,8 +388,13 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         const AppDef &def = app_def(jobs[i].app);
         P->apps.push_back(jobs[i].app);
         P->graphs.push_back(jobs[i].graph);  // an oriented view is owned by (and freed with) its source
-        for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
-        const int engine = pick_engine(ctx->cfg, def, jobs[i].app, *get_graph(ctx, jobs[i].graph));
+        const int64_t lab = start_labels ? start_labels[i] : -1;
+        const Graph &g0 = *get_graph(ctx, jobs[i].graph);
+        const StartFilter sf = lab >= 0 ? StartFilter{g0.labels, (uint32_t)lab} : StartFilter{nullptr, 0};
+        const uint64_t starts = lab >= 0 ? g0.label_count[(size_t)lab] : g0.n;  // depth-0 extensions
+        if (lab < 0)
+            for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
+        const int engine = pick_engine(ctx->cfg, def, jobs[i].app, g0, lab >= 0);
         if (engine == KHZ_ENGINE_BITMAP && !def.clique) {
             // 3-motif: triangles on the oriented view (bitmap engine, k = 3) + degree sums
             const Graph sg = *get_graph(ctx, jobs[i].graph);
@@ -385,7 +407,8 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             bm_entries += og->m;
             bmax = std::max(bmax, og->max_degree);
             if (og->max_degree > bitmap_block_max_degree())
-                add_dfs(*og, app_def(KHZ_KAUTO_TRIANGLE).plans[0], i, bitmap_block_max_degree() + 1);
+                add_dfs(*og, app_def(KHZ_KAUTO_TRIANGLE).plans[0], i, bitmap_block_max_degree() + 1,
+                        StartFilter{nullptr, 0});
             const bool kauto = jobs[i].app == KHZ_KAUTO_3MOTIF;
             mjobs.push_back(MJob{sg.off, sg.n, (uint32_t)i, kauto ? 1 : 0, 0});
             // the bitmap launch adds one level-1 extension per undirected edge; kautomine's fused run
@@ -396,26 +419,28 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             Graph *og = nullptr;
             khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
             if (st) return st;
+            // restricted: og is the graph as stored (pick_engine), so its labels apply
             BJob b{og->off, og->adj, og->n, def.clique_k, vbase, (uint32_t)i,
-                   bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m), nullptr};
+                   bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m), nullptr, sf};
             bjobs.push_back(b);
             vbase += og->n;
             bm_entries += og->m;
             bmax = std::max(bmax, og->max_degree);
             if (og->max_degree > bitmap_block_max_degree())
-                add_dfs(*og, def.plans[0], i, bitmap_block_max_degree() + 1);
-            ext_add[i] = og->n;
+                add_dfs(*og, def.plans[0], i, bitmap_block_max_degree() + 1, sf);
+            ext_add[i] = lab >= 0 ? starts : og->n;
             P->engine = KHZ_ENGINE_BITMAP;
         } else if (engine == KHZ_ENGINE_WEDGE) {
             const Graph &g = *get_graph(ctx, jobs[i].graph);
-            wjobs.push_back(WJob{g.off, g.adj, g.n, g.max_degree, wbase, (uint32_t)i, 0});
+            wjobs.push_back(WJob{g.off, g.adj, g.n, g.max_degree, wbase, (uint32_t)i, 0, sf});
             wbase += g.n;
-            ext_add[i] = (uint64_t)g.n + g.m / 2;  // depth 0 and every undirected edge once at depth 1
+            // depth 0 and every undirected edge once at depth 1 (restricted: depth 1 counted on the device)
+            ext_add[i] = lab >= 0 ? starts : (uint64_t)g.n + g.m / 2;
             if (P->engine == KHZ_ENGINE_DFS) P->engine = KHZ_ENGINE_WEDGE;
         } else {
             const Graph &g = *get_graph(ctx, jobs[i].graph);
-            for (int r = 0; r < def.num_runs; ++r) add_dfs(g, def.plans[r], i, 0);
-            ext_add[i] = (uint64_t)g.n * def.num_runs;
+            for (int r = 0; r < def.num_runs; ++r) add_dfs(g, def.plans[r], i, 0, sf);
+            ext_add[i] = starts * def.num_runs;
         }
     }
     P->has_bitmap = !bjobs.empty();
@@ -564,10 +589,11 @@ khz_status fill_stats(khz_ctx *ctx, BatchPlan *P, const LaunchStats &ls, bool ti
 }
 
 // the cached prepared launch of one (graph, app) under the current configuration
-khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, BatchPlan **out) {
-    char key[160];
-    snprintf(key, sizeof(key), "%u/%d/%d/%d/%d/%d/%d/%d", g, app, ctx->cfg.engine, ctx->cfg.want_algo_bytes,
-             ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, ctx->cfg.bitmap_warp_max, ctx->cfg.bitmap_hub_rows);
+khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, BatchPlan **out, int64_t start_label = -1) {
+    char key[192];
+    snprintf(key, sizeof(key), "%u/%d/%d/%d/%d/%d/%d/%d/%lld", g, app, ctx->cfg.engine, ctx->cfg.want_algo_bytes,
+             ctx->cfg.dfs_warps_per_sm, ctx->cfg.dfs_chunk, ctx->cfg.bitmap_warp_max, ctx->cfg.bitmap_hub_rows,
+             (long long)start_label);
     auto it = ctx->plans.find(key);
     if (it != ctx->plans.end()) {
         *out = it->second.get();
@@ -575,7 +601,7 @@ khz_status cached_plan(khz_ctx *ctx, khz_graph g, int app, cudaStream_t s, Batch
     }
     khz_job j{g, (int32_t)app, 0};
     std::unique_ptr<BatchPlan> P;
-    khz_status st = build_plan(ctx, &j, 1, s, kPlanPoolMem | kPlanFreeLegacy, &P);
+    khz_status st = build_plan(ctx, &j, 1, s, kPlanPoolMem | kPlanFreeLegacy, &P, &start_label);
     if (st) return st;
     *out = P.get();
     ctx->plans[key] = std::move(P);
@@ -946,7 +972,18 @@ khz_status khz_graph_load_dgraph(khz_ctx *ctx, const char *path, uint32_t flags,
         set_error("%s: edge labels are not supported (graph_loader.h:750)", path);
         return KHZ_ERR_FORMAT;
     }
-    if (has_label) fseek(f, 20 + 4 * (long)n, SEEK_SET);
+    std::vector<uint32_t> labels;
+    const bool keep_labels = has_label && !(flags & (KHZ_SKIP_LABELS | KHZ_ORIENT));
+    if (keep_labels) {
+        labels.resize(n);
+        if (n > 0 && fread(labels.data(), 4, n, f) != n) {
+            fclose(f);
+            set_error("%s: truncated label section", path);
+            return KHZ_ERR_FORMAT;
+        }
+    } else if (has_label) {
+        fseek(f, 20 + 4 * (long)n, SEEK_SET);
+    }
     uint32_t *pairs = nullptr;
     if (m > 0 && cudaMallocHost(&pairs, sizeof(uint32_t) * 2 * m) != cudaSuccess) {
         cudaGetLastError();
@@ -963,6 +1000,15 @@ khz_status khz_graph_load_dgraph(khz_ctx *ctx, const char *path, uint32_t flags,
     }
     khz_status st = khz_graph_from_edges(ctx, pairs, m, n, flags & ~KHZ_EDGES_ON_DEVICE, out, nullptr);
     if (pairs) cudaFreeHost(pairs);
+    if (st == KHZ_OK && keep_labels) {
+        st = khz_graph_set_labels(ctx, *out, labels.data(), n);
+        if (st != KHZ_OK) {
+            const std::string why = khz_last_error_string();
+            khz_graph_free(ctx, *out);
+            *out = 0;
+            set_error("%s: %s", path, why.c_str());
+        }
+    }
     return st;
 }
 
@@ -1028,6 +1074,8 @@ khz_status khz_graph_info_get(khz_ctx *ctx, khz_graph h, khz_graph_info *info) {
     info->d_offsets = g->off;
     info->d_adj = g->adj;
     info->device_bytes = g->bytes;
+    info->num_labels = g->num_labels;
+    info->d_labels = g->labels;
     return KHZ_OK;
 }
 
@@ -1082,6 +1130,72 @@ khz_status khz_graph_write_dgraph(khz_ctx *ctx, khz_graph h, const char *path, c
         set_error("short write to %s", path);
         return KHZ_ERR_FORMAT;
     }
+    return KHZ_OK;
+}
+
+khz_status khz_graph_set_labels(khz_ctx *ctx, khz_graph h, const uint32_t *labels, uint32_t num_vertices) {
+    khz_status st = check_ctx(ctx);
+    if (st) return st;
+    if (!labels && num_vertices > 0) {
+        set_error("null labels");
+        return KHZ_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    Graph *g = get_graph(ctx, h);
+    if (!g) return KHZ_ERR_ARG;
+    if (num_vertices != g->n) {
+        set_error("%u labels given for a graph of %u vertices", num_vertices, g->n);
+        return KHZ_ERR_ARG;
+    }
+    // dense labels (graph_loader.h:784-804): num_labels = max + 1, every label used
+    uint32_t mx = 0;
+    for (uint32_t v = 0; v < num_vertices; ++v) mx = std::max(mx, labels[v]);
+    if (num_vertices > 0 && mx == 0xffffffffu) {
+        set_error("label 0xffffffff is out of range");
+        return KHZ_ERR_FORMAT;
+    }
+    std::vector<uint64_t> cnt(num_vertices > 0 ? (size_t)mx + 1 : 0, 0);
+    if (cnt.size() > (size_t)num_vertices) {
+        set_error("the vertex labels should be continuous and range from 0 to num_labels - 1 (largest %u, %u vertices)",
+                  mx, num_vertices);
+        return KHZ_ERR_FORMAT;
+    }
+    for (uint32_t v = 0; v < num_vertices; ++v) cnt[labels[v]] += 1;
+    for (size_t l = 0; l < cnt.size(); ++l) {
+        if (cnt[l] == 0) {
+            set_error("the vertex labels should be continuous and range from 0 to num_labels - 1 (label %zu unused)", l);
+            return KHZ_ERR_FORMAT;
+        }
+    }
+    KHZ_CUDA(cudaDeviceSynchronize());  // launches in flight may read the previous labels
+    // prepared launches hold the label pointer: drop the graph's
+    for (auto it = ctx->plans.begin(); it != ctx->plans.end();) {
+        const auto &gs = it->second->graphs;
+        if (std::find(gs.begin(), gs.end(), h) != gs.end()) it = ctx->plans.erase(it);
+        else ++it;
+    }
+    AllocScope scope(ctx->pool, nullptr);
+    dev_free(g->labels);
+    g->labels = nullptr;
+    g->num_labels = 0;
+    g->label_count.clear();
+    if (num_vertices == 0) return KHZ_OK;
+    void *d = nullptr;
+    cudaError_t e = dev_alloc(&d, sizeof(uint32_t) * num_vertices);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation for %u labels failed", num_vertices);
+        return KHZ_ERR_OOM;
+    }
+    e = cudaMemcpyAsync(d, labels, sizeof(uint32_t) * num_vertices, cudaMemcpyHostToDevice, nullptr);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(nullptr);
+    if (e != cudaSuccess) {
+        dev_free(d);
+        return cuda_fail(e, "label upload");
+    }
+    g->labels = (uint32_t *)d;
+    g->num_labels = (uint32_t)cnt.size();
+    g->label_count = std::move(cnt);
     return KHZ_OK;
 }
 
@@ -1148,17 +1262,26 @@ khz_status khz_count_async(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *
     return KHZ_OK;
 }
 
-khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts, khz_stats *stats, void *stream) {
+}  // extern "C"
+
+namespace {
+// khz_count and khz_count_restricted (start_label < 0: every start vertex)
+khz_status count_one(khz_ctx *ctx, khz_graph g, khz_app_id app, int64_t start_label, uint64_t *counts,
+                     khz_stats *stats, void *stream) {
     khz_status st = check_ctx(ctx);
     if (st) return st;
     if (!counts) {
         set_error("null counts");
         return KHZ_ERR_ARG;
     }
+    if (app < 0 || app >= KHZ_NUM_APPS) {
+        set_error("invalid app id %d", (int)app);
+        return KHZ_ERR_ARG;
+    }
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = (cudaStream_t)stream;
     BatchPlan *P = nullptr;
-    st = cached_plan(ctx, g, app, s, &P);
+    st = cached_plan(ctx, g, app, s, &P, start_label);
     if (st) return st;
     st = ensure_shared(ctx, P->slot_words);
     if (st) return st;
@@ -1173,6 +1296,18 @@ khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts
     for (int c = 0; c < nc; ++c) counts[c] = P->h_final[c];
     if (stats) return fill_stats(ctx, P, ls, true, stats);
     return KHZ_OK;
+}
+}  // namespace
+
+extern "C" {
+
+khz_status khz_count(khz_ctx *ctx, khz_graph g, khz_app_id app, uint64_t *counts, khz_stats *stats, void *stream) {
+    return count_one(ctx, g, app, -1, counts, stats, stream);
+}
+
+khz_status khz_count_restricted(khz_ctx *ctx, khz_graph g, khz_app_id app, uint32_t start_label, uint64_t *counts,
+                                khz_stats *stats, void *stream) {
+    return count_one(ctx, g, app, (int64_t)start_label, counts, stats, stream);
 }
 
 khz_status khz_count_batch(khz_ctx *ctx, const khz_job *jobs, int n_jobs, uint64_t *counts, uint64_t *num_ext,

@@ -83,6 +83,20 @@ struct Graph {
     uint32_t *adj = nullptr; // device m + kAdjPad
     khz_graph oriented_view = 0;  // cached orientation of a symmetric graph (owned)
     uint64_t bytes = 0;
+    // optional node labels (the .dgraph label section, graph_loader.h:773-822): device n uint32,
+    // labels dense in [0, num_labels), and the number of vertices of each label (host)
+    uint32_t *labels = nullptr;
+    uint32_t num_labels = 0;
+    std::vector<uint64_t> label_count;
+};
+
+// Start-vertex restriction of one job (run(..., restrict_starting_vertex_label, label),
+// engine.cc:1457-1496): only start vertices v_0 with labels[v_0] == label are extended.
+// labels == nullptr: every start vertex.
+struct StartFilter {
+    const uint32_t *labels;
+    uint32_t label;
+    __device__ __forceinline__ bool keep(uint32_t v0) const { return labels == nullptr || __ldg(labels + v0) == label; }
 };
 
 // DFS job (one (graph, plan) run inside a launch)
@@ -95,6 +109,7 @@ struct DfsJob {
     uint64_t num_units;    // = CSR entries (one level-1 candidate per unit)
     uint32_t out_base;     // counter row (KHZ_MAX_COUNTS + 2 uint64 per job)
     uint32_t min_deg;      // skip start vertices whose degree is below this (handled elsewhere)
+    StartFilter start;     // start-vertex label restriction
 };
 
 constexpr int kRowWords = KHZ_MAX_COUNTS + 2;  // counter row: counts[6], NumExtensions, algorithmic bytes
@@ -110,6 +125,7 @@ struct BJob {
     uint32_t out_row;
     uint32_t hub_rows;  // rows H of the hub triangle (vertices n - H .. n - 1), 0 = none
     const uint32_t *hub;  // the triangle (set by bitmap_prepare)
+    StartFilter start;    // start-vertex label restriction
 };
 
 // bump allocator over one device allocation
@@ -154,6 +170,7 @@ struct WJob {
     uint64_t vbase;
     uint32_t out_row;
     uint32_t pad2;
+    StartFilter start;  // start-vertex label restriction (then the level-1 extensions are counted on the device)
 };
 
 struct WedgeLaunch {

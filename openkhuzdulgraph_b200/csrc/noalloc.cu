@@ -8,7 +8,7 @@
 // The caller still provides the graph (device CSR) and the output buffer.
 //
 // The array is part of the library's device image: every GPU that loads the library holds
-// it (kNoAllocBytes, about 14.6 MiB) until the process exits.  Its size fixes the limits:
+// it (kNoAllocBytes = 14,557,184 bytes, about 13.9 MiB) until the process exits.  Its size fixes the limits:
 // at most kNoAllocWarps resident warps, and no vertex of degree above kNoAllocMaxDegree.
 #include <cuda_runtime.h>
 

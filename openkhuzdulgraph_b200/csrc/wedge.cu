@@ -64,8 +64,12 @@ __global__ void wedge_classify_kernel(const WJob *__restrict__ jobs, int n_jobs,
         const int j = wjob_of(jobs, n_jobs, gv);
         const WJob &J = jobs[j];
         const uint32_t v0 = (uint32_t)(gv - J.vbase);
+        if (!J.start.keep(v0)) continue;
         const uint64_t b = J.off[v0], e = J.off[v0 + 1];
         const uint32_t start = upper_bound_u32(J.adj + b, 0, (uint32_t)(e - b), v0);
+        // with a start-vertex restriction the level-1 extensions (v1 > v0) are counted here
+        if (J.start.labels && lane == 0 && e - b > start)
+            atomicAdd((unsigned long long *)&wrow(rows, J)[KHZ_MAX_COUNTS], (unsigned long long)(e - b - start));
         uint64_t wedges = 0;
         for (uint64_t i = b + start + lane; i < e; i += 32) {
             const uint32_t w = J.adj[i];

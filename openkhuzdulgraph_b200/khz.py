@@ -29,6 +29,7 @@ MAX_COUNTS = 6
 EDGES_ON_DEVICE = 0x1
 ORIENT = 0x2
 UNCHECKED = 0x4
+SKIP_LABELS = 0x8
 
 ENGINE_AUTO, ENGINE_DFS, ENGINE_BITMAP, ENGINE_WEDGE = 0, 1, 2, 3
 
@@ -43,7 +44,8 @@ STATUS = {0: "KHZ_OK", 1: "KHZ_ERR_ARG", 2: "KHZ_ERR_OOM", 3: "KHZ_ERR_OVERFLOW"
 EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_get_config",
            "khz_last_error_string", "khz_abi_version", "khz_graph_from_edges", "khz_graph_load_dgraph",
            "khz_graph_orient", "khz_graph_generate_rmat", "khz_graph_info_get", "khz_graph_export_csr",
-           "khz_graph_write_dgraph", "khz_graph_free", "khz_count", "khz_count_async", "khz_app_num_counts",
+           "khz_graph_write_dgraph", "khz_graph_set_labels", "khz_graph_free", "khz_count", "khz_count_async",
+           "khz_count_restricted", "khz_app_num_counts",
            "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch", "khz_count_noalloc",
            "khz_batch_create", "khz_batch_launch", "khz_batch_wait", "khz_batch_destroy",
            "khz_server_create", "khz_server_submit", "khz_server_wait", "khz_server_stats_get",
@@ -59,7 +61,8 @@ class KhzError(RuntimeError):
 class GraphInfo(ctypes.Structure):
     _fields_ = [("num_vertices", ctypes.c_uint32), ("max_degree", ctypes.c_uint32),
                 ("num_entries", ctypes.c_uint64), ("oriented", ctypes.c_int32), ("symmetric", ctypes.c_int32),
-                ("d_offsets", ctypes.c_void_p), ("d_adj", ctypes.c_void_p), ("device_bytes", ctypes.c_uint64)]
+                ("d_offsets", ctypes.c_void_p), ("d_adj", ctypes.c_void_p), ("device_bytes", ctypes.c_uint64),
+                ("num_labels", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("d_labels", ctypes.c_void_p)]
 
 
 class Stats(ctypes.Structure):
@@ -130,9 +133,11 @@ def lib():
             "khz_graph_info_get": (i32, [vp, u32, P(GraphInfo)]),
             "khz_graph_export_csr": (i32, [vp, u32, vp, vp]),
             "khz_graph_write_dgraph": (i32, [vp, u32, ctypes.c_char_p, vp]),
+            "khz_graph_set_labels": (i32, [vp, u32, vp, u32]),
             "khz_graph_free": (i32, [vp, u32]),
             "khz_count": (i32, [vp, u32, i32, P(u64), P(Stats), vp]),
             "khz_count_async": (i32, [vp, u32, i32, vp, vp]),
+            "khz_count_restricted": (i32, [vp, u32, i32, u32, P(u64), P(Stats), vp]),
             "khz_app_num_counts": (i32, [i32]),
             "khz_app_multiplicity": (i32, [i32, i32]),
             "khz_count_batch": (i32, [vp, P(Job), i32, P(u64), P(u64), P(Stats), vp]),
@@ -201,6 +206,11 @@ class Graph:
         _check(lib().khz_graph_orient(self.ctx.ptr, self.handle, ctypes.byref(h), stream))
         return Graph(self.ctx, h.value)
 
+    def set_labels(self, labels):
+        """Node labels (one uint32 per vertex, dense in [0, num_labels))."""
+        labels = np.ascontiguousarray(labels, dtype=np.uint32)
+        _check(lib().khz_graph_set_labels(self.ctx.ptr, self.handle, labels.ctypes.data, labels.shape[0]))
+
     def write_dgraph(self, path, labels=None):
         lab = None
         if labels is not None:
@@ -260,9 +270,11 @@ class Context:
         _check(lib().khz_graph_from_edges(self.ptr, ptr, m, n, flags, ctypes.byref(h), stream))
         return Graph(self, h.value)
 
-    def load_dgraph(self, path, orient=False):
+    def load_dgraph(self, path, orient=False, labels=True):
+        """labels=False: ignore the file's node labels (load_vertex_labels = false)."""
         h = ctypes.c_uint32(0)
-        _check(lib().khz_graph_load_dgraph(self.ptr, path.encode(), ORIENT if orient else 0, ctypes.byref(h)))
+        flags = (ORIENT if orient else 0) | (0 if labels else SKIP_LABELS)
+        _check(lib().khz_graph_load_dgraph(self.ptr, path.encode(), flags, ctypes.byref(h)))
         return Graph(self, h.value)
 
     def generate_rmat(self, scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=1, orient=False, stream=None):
@@ -277,6 +289,15 @@ class Context:
         counts = (ctypes.c_uint64 * MAX_COUNTS)()
         st = Stats()
         _check(lib().khz_count(self.ptr, graph.handle, aid, counts, ctypes.byref(st), stream))
+        return [int(counts[i]) for i in range(num_counts(aid))], st
+
+    def count_restricted(self, graph, app, label, stream=None):
+        """run(..., restrict_starting_vertex_label=True, label): (raw counts list, Stats) over the
+        start vertices whose label is `label`; counts are not divided by the multiplicities."""
+        aid = _app_id(app)
+        counts = (ctypes.c_uint64 * MAX_COUNTS)()
+        st = Stats()
+        _check(lib().khz_count_restricted(self.ptr, graph.handle, aid, label, counts, ctypes.byref(st), stream))
         return [int(counts[i]) for i in range(num_counts(aid))], st
 
     def count_async(self, graph, app, d_out_ptr, stream=None):

@@ -696,8 +696,12 @@ static int num_runs(int app) {
     return 1;
 }
 
-int orc_count(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, uint32_t v0_mod, uint32_t v0_rem,
-              int threads, uint64_t *counts, uint64_t *num_ext, uint64_t *algo_bytes) {
+/* Start vertices: v0 % v0_mod == v0_rem, and, when labels is given, labels[v0] == label (the
+ * restrict_starting_vertex_label run of WorkloadDistributer::fetch_next_batch_local,
+ * engine.cc:1457-1496).  raw: keep the aggregators' raw values (no multiplicity division). */
+static int count_impl(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *labels,
+                      uint32_t label, uint32_t v0_mod, uint32_t v0_rem, int threads, int raw, uint64_t *counts,
+                      uint64_t *num_ext, uint64_t *algo_bytes) {
     if (app < 0 || app >= ORC_NUM_APPS || v0_mod == 0) return -1;
     uint32_t maxd = 0;
     for (uint32_t v = 0; v < n; ++v) { uint32_t d = (uint32_t)(off[v + 1] - off[v]); if (d > maxd) maxd = d; }
@@ -714,6 +718,7 @@ int orc_count(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, uin
             orc_tc *t = &tc;
 #pragma omp for schedule(dynamic, 64)
             for (uint32_t v0 = v0_rem; v0 < n; v0 += v0_mod) {
+                if (labels && labels[v0] != label) continue;
                 switch (app) {
                     case ORC_KAUTO_TRIANGLE: kauto_triangle(t, v0); break;
                     case ORC_KAUTO_4CLIQUE: kauto_clique(t, v0, 4); break;
@@ -737,11 +742,12 @@ int orc_count(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, uin
         }
     }
     /* multiplicities: kautomine/three_motif.cc:44 ({1, 2}); 4-motif {1, 2, 1, 8, 1, 1} */
-    if (app == ORC_KAUTO_3MOTIF) {
+    if (raw) {
+        /* the aggregators' values as they are */
+    } else if (app == ORC_KAUTO_3MOTIF) {
         if (tot[1] % 2) return -2;
         tot[1] /= 2;
-    }
-    if (app == ORC_KAUTO_4MOTIF) {
+    } else if (app == ORC_KAUTO_4MOTIF) {
         if (tot[1] % 2 || tot[3] % 8) return -2;
         tot[1] /= 2;
         tot[3] /= 8;
@@ -750,6 +756,17 @@ int orc_count(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, uin
     if (num_ext) *num_ext = ext;
     if (algo_bytes) *algo_bytes = bytes;
     return 0;
+}
+
+int orc_count(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, uint32_t v0_mod, uint32_t v0_rem,
+              int threads, uint64_t *counts, uint64_t *num_ext, uint64_t *algo_bytes) {
+    return count_impl(app, n, off, adj, NULL, 0, v0_mod, v0_rem, threads, 0, counts, num_ext, algo_bytes);
+}
+
+int orc_count_labeled(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *labels,
+                      uint32_t label, int threads, uint64_t *raw_counts, uint64_t *num_ext, uint64_t *algo_bytes) {
+    if (!labels) return -1;
+    return count_impl(app, n, off, adj, labels, label, 1, 0, threads, 1, raw_counts, num_ext, algo_bytes);
 }
 
 /* ------------------------------------------------------------------------- */

@@ -85,6 +85,11 @@ uint32_t orc_trim_lower_bound(const uint32_t *a, uint32_t na, uint32_t lower_bou
 int orc_num_counts(int app);
 int orc_count(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, uint32_t v0_mod, uint32_t v0_rem,
               int threads, uint64_t *counts, uint64_t *num_ext, uint64_t *algo_bytes);
+/* The run restricted to the start vertices whose label is `label` (run(..., true, label),
+ * distributed_application.h:54, engine.cc:1457-1496); raw_counts are the aggregators' values
+ * before any multiplicity division. */
+int orc_count_labeled(int app, uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *labels,
+                      uint32_t label, int threads, uint64_t *raw_counts, uint64_t *num_ext, uint64_t *algo_bytes);
 
 /* ---- brute force (small graphs only) ----
  * Counts subgraph copies by enumerating vertex subsets.  pattern ids:

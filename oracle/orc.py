@@ -33,8 +33,22 @@ _lib = None
 def build():
     """Compile liborc.so (and, when the reference tree is present, oracle/_ref)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "liborc.so"])
-    if os.path.isdir("/root/reference"):
-        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref"])
+    ref = reference_tree()
+    if ref:
+        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", "REF=" + ref])
+
+
+def reference_tree():
+    """The reference source tree the recipe compiles oracle/_ref from: $KHZ_REF, else the
+    default checkout location named in oracle/Makefile; None when absent (as on a machine
+    that only runs the prebuilt files)."""
+    path = os.environ.get("KHZ_REF")
+    if not path:
+        with open(os.path.join(HERE, "Makefile")) as f:
+            for line in f:
+                if line.startswith("KHZ_REF ?="):
+                    path = line.split("?=", 1)[1].strip()
+    return path if path and os.path.isdir(path) else None
 
 
 def lib():
@@ -77,6 +91,10 @@ def lib():
         L.orc_count.argtypes = [ctypes.c_int, ctypes.c_uint32, _u64p, _u32p, ctypes.c_uint32, ctypes.c_uint32,
                                 ctypes.c_int, _u64p, ctypes.POINTER(ctypes.c_uint64),
                                 ctypes.POINTER(ctypes.c_uint64)]
+        L.orc_count_labeled.restype = ctypes.c_int
+        L.orc_count_labeled.argtypes = [ctypes.c_int, ctypes.c_uint32, _u64p, _u32p, _u32p, ctypes.c_uint32,
+                                        ctypes.c_int, _u64p, ctypes.POINTER(ctypes.c_uint64),
+                                        ctypes.POINTER(ctypes.c_uint64)]
         L.orc_brute.restype = ctypes.c_uint64
         L.orc_brute.argtypes = [ctypes.c_int, ctypes.c_uint32, _u64p, _u32p]
         _lib = L
@@ -144,6 +162,25 @@ def count(app, off, adj, v0_mod=1, v0_rem=0, threads=0):
                          ctypes.byref(ne), ctypes.byref(nb))
     if rc != 0:
         raise RuntimeError("orc_count failed (%d)" % rc)
+    return [int(x) for x in counts[:nc]], ne.value, nb.value
+
+
+def count_labeled(app, off, adj, labels, label, threads=0):
+    """(raw counts, num_extensions, algorithmic bytes) of the run restricted to the start vertices
+    whose label is `label`; counts are not divided by the multiplicities."""
+    aid = APPS[app] if isinstance(app, str) else int(app)
+    nc = lib().orc_num_counts(aid)
+    counts = np.zeros(6, dtype=np.uint64)
+    ne = ctypes.c_uint64(0)
+    nb = ctypes.c_uint64(0)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    if adj.shape[0] == 0:
+        adj = np.zeros(1, dtype=np.uint32)
+    labels = np.ascontiguousarray(labels, dtype=np.uint32)
+    rc = lib().orc_count_labeled(aid, off.shape[0] - 1, off, adj, labels, label, threads, counts,
+                                 ctypes.byref(ne), ctypes.byref(nb))
+    if rc != 0:
+        raise RuntimeError("orc_count_labeled failed (%d)" % rc)
     return [int(x) for x in counts[:nc]], ne.value, nb.value
 
 

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_metadata_without_gpu():
     L = khz.lib()
-    assert L.khz_abi_version() == 1
+    assert L.khz_abi_version() == 2
     assert [khz.num_counts(a) for a in range(12)] == [1, 1, 1, 2, 1, 1, 1, 2, 1, 1, 1, 6]
     assert L.khz_app_multiplicity(3, 1) == 2
     assert [L.khz_app_multiplicity(11, p) for p in range(6)] == [1, 2, 1, 8, 1, 1]
@@ -57,3 +57,11 @@ def test_config_layout_is_fixed():
     import ctypes
     assert ctypes.sizeof(khz.Config) == 64
     assert khz.Config.bitmap_hub_rows.offset == 24 and khz.Config.reserved.offset == 28
+
+
+def test_graph_info_layout():
+    """khz_graph_info (ABI version 2): the label fields follow device_bytes."""
+    import ctypes
+    assert ctypes.sizeof(khz.GraphInfo) == 64
+    assert khz.GraphInfo.device_bytes.offset == 40 and khz.GraphInfo.num_labels.offset == 48
+    assert khz.GraphInfo.d_labels.offset == 56

@@ -82,6 +82,42 @@ def test_oracle_matches_reference_sampled_driver(golden, app):
         assert ext == ref["num_extensions"], (spec["name"], app)
 
 
+@pytest.mark.parametrize("app", orc.REF_APPS)
+def test_labeled_oracle_matches_reference_sampled_driver(golden, app):
+    """The label-restricted run (raw aggregator values) against the reference's own sampled driver,
+    which runs the app with restrict_starting_vertex_label on labels v % mod."""
+    mod, rem = golden["sample"]["mod"], golden["sample"]["rem"]
+    aid = orc.APPS[app]
+    for spec in golden["graphs"]:
+        ref = spec["apps_sampled"].get(app)
+        if ref is None:
+            continue
+        _, n, _, off, adj = golden_graph(spec)
+        labels = (np.arange(n, dtype=np.uint64) % mod).astype(np.uint32)
+        raw, ext, _ = orc.count_labeled(app, off, adj, labels, rem, threads=2)
+        mult = [2 if (aid == 3 and p == 1) else 1 for p in range(len(raw))]
+        assert [r // m for r, m in zip(raw, mult)] == ref["counts"], (spec["name"], app)
+        assert ext == ref["num_extensions"], (spec["name"], app)
+
+
+def test_label_slices_partition_the_whole_count():
+    """Summed over all labels, the restricted runs give the unrestricted raw counts and NumExtensions."""
+    canon, n = orc.er(300, 2500, seed=5)
+    off, adj = orc.csr(orc.symmetrize(canon), n)
+    labels = (np.arange(n, dtype=np.uint64) * 7919 % 5).astype(np.uint32)
+    for app in orc.APPS:
+        whole, ext, _ = orc.count(app, off, adj, threads=2)
+        aid = orc.APPS[app]
+        mult = {3: [1, 2], 11: [1, 2, 1, 8, 1, 1]}.get(aid, [1] * len(whole))
+        tot, tot_ext = [0] * len(whole), 0
+        for lab in range(5):
+            raw, e, _ = orc.count_labeled(app, off, adj, labels, lab, threads=2)
+            tot = [a + b for a, b in zip(tot, raw)]
+            tot_ext += e
+        assert [t // m for t, m in zip(tot, mult)] == whole, app
+        assert tot_ext == ext, app
+
+
 # brute-force pattern ids (khz_oracle.h) for each app's counts
 BRUTE = {
     "kautomine_triangle": [0], "kautomine_four_clique": [1], "kautomine_five_clique": [2],

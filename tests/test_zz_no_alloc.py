@@ -50,6 +50,46 @@ def test_no_alloc_matches_regular_entry_point():
             g.free()
 
 
+def test_no_alloc_at_its_degree_limit_allocates_nothing():
+    """A graph whose largest degree is exactly the limit (a star of 1024 leaves, consecutive leaves
+    joined into triangles with the centre, plus a few chords) fills every warp slot to capacity; the
+    counts must still be the regular entry point's, and the device's free memory must not change
+    across the calls (after the first, which may load the library's device code)."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from openkhuzdulgraph_b200 import khz
+    leaves = 1024
+    pairs = [(0, v) for v in range(1, leaves + 1)]
+    pairs += [(v, v + 1) for v in range(1, leaves, 2)]
+    pairs += [(v, v + 7) for v in range(2, leaves - 7, 37)]
+    canon = np.array(sorted(set(pairs)), dtype=np.uint32)
+    sym = orc.symmetrize(canon)
+    with khz.Context(0) as ctx:
+        ctx.set_config(engine=khz.ENGINE_DFS)
+        g = ctx.graph_from_edges(sym, leaves + 1)
+        gi = g.info()
+        assert gi.max_degree == 1024
+        d_out = torch.zeros(8, dtype=torch.int64, device="cuda")
+        expected = {app: ctx.count(g, app) for app in APPS}
+        khz.count_noalloc(gi.d_offsets, gi.d_adj, gi.num_vertices, gi.num_entries, 0, d_out.data_ptr())
+        torch.cuda.synchronize()
+        free_before, _ = torch.cuda.mem_get_info()
+        for app in APPS:
+            exp_counts, st = expected[app]
+            nc = khz.num_counts(app)
+            for _ in range(2):
+                d_out.fill_(-1)
+                khz.count_noalloc(gi.d_offsets, gi.d_adj, gi.num_vertices, gi.num_entries, app, d_out.data_ptr())
+                got = d_out.cpu().numpy().view(np.uint64)
+                assert [int(x) for x in got[:nc]] == exp_counts, app
+                assert int(got[6]) == st.num_extensions, app
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info()
+        assert free_after == free_before
+        g.free()
+
+
 def test_no_alloc_rejects_degrees_beyond_its_limit():
     import torch
     if not torch.cuda.is_available():
