@@ -33,9 +33,10 @@ typedef enum khz_status {
     KHZ_ERR_FORMAT = 6,   /* input graph violates the .dgraph contract */
     KHZ_ERR_BUSY = 7,     /* serving queue full / ticket not finished */
     KHZ_ERR_NOT_FOUND = 8,
-    KHZ_ERR_MULTIPLICITY = 9 /* a raw count is not divisible by the pattern multiplicity: the input
-                                is not the undirected graph the app assumes (the reference asserts,
-                                kautomine/three_motif.cc:232,243) */
+    KHZ_ERR_MULTIPLICITY = 9, /* a raw count is not divisible by the pattern multiplicity: the input
+                                 is not the undirected graph the app assumes (the reference asserts,
+                                 kautomine/three_motif.cc:232,243) */
+    KHZ_ERR_CANCELLED = 10    /* a served query was withdrawn before it ran (khz_server_cancel) */
 } khz_status;
 
 /* Pattern applications; the numbering is shared with the oracle.
@@ -110,7 +111,10 @@ typedef struct khz_config {
     int32_t bitmap_hub_rows;   /* bitmap engine: rows of the hub adjacency triangle over the
                                   highest-ranked vertices (0 = auto, -1 = none, else rounded down
                                   to a multiple of 32 and capped at the vertex count) */
-    int32_t reserved[9];
+    int32_t device_mem_limit_mib; /* cap on the device memory the context holds for graphs and counting
+                                     scratch, in MiB (0 = none): an allocation that would exceed it
+                                     fails with KHZ_ERR_OOM, as if the device were that small */
+    int32_t reserved[8];
 } khz_config;
 
 /* ---- context ---------------------------------------------------------------------- */
@@ -181,6 +185,64 @@ int khz_app_num_counts(khz_app_id app);
 /* mirrors the reference's `multiplicities[]` tables (kautomine/three_motif.cc:44) */
 int khz_app_multiplicity(khz_app_id app, int pattern);
 
+/* ---- apps that bring their own schedule ------------------------------------------ */
+/* Replaces the ApplyFunction contract (engine.h:589) and the engine calls an apply() makes
+ * (scatter / cached objects, engine.h:592-613, 846-859): an app describes its apply() levels as
+ * data, and the DFS engine runs them on the device.  Level l binds vertex v_l (l = 1 .. k-2
+ * enumerate, level k-1 counts).  A level's candidate set is `base op0 N(v_a) op1 N(v_b)`:
+ *   base = N(v_i) (KHZ_BASE_NBR, arg i) or a set materialised earlier (KHZ_BASE_SET, arg 2 or 3 =
+ *          the set of level 2 or 3, arg 4 = the level's cached set), op = intersect_with (AND) or
+ *          subtracted_by (SUB) of the vertex_set.cc routines;
+ * the filters are the generated code's `v > v_a` restrictions (gt_mask: keep x above every v_a of
+ * the mask) and `v != v_a` exclusions (ne_mask, at most 4 bits); a level's set is materialised
+ * (the reference's cached prefix) when it has an op; `cached` is computed when the level is
+ * entered, as an apply() computes a cached object for its children.  The last level adds
+ * |set passing its filters| to its counter (1 or 2 counting terms: compute-fused apps), optionally
+ * only when v[guard_lo] < v[guard_hi].  `finalized` levels do not count towards NumExtensions
+ * (a finalized scatter, engine.cc:1441-1452).  Level 1 must enumerate N(v_0) itself. */
+#define KHZ_BASE_NBR 0
+#define KHZ_BASE_SET 1
+#define KHZ_OP_NONE 0
+#define KHZ_OP_AND 1
+#define KHZ_OP_SUB 2
+typedef struct khz_set_expr {
+    int8_t base_kind;  /* KHZ_BASE_NBR or KHZ_BASE_SET */
+    int8_t base_arg;   /* vertex index, or set 2 / 3 / 4 */
+    int8_t op[2];      /* KHZ_OP_* */
+    int8_t op_arg[2];  /* vertex index b of N(v_b) */
+} khz_set_expr;
+typedef struct khz_term {
+    khz_set_expr set;
+    uint8_t gt_mask;
+    uint8_t ne_mask;
+    int8_t guard_lo, guard_hi; /* -1: unguarded */
+    int8_t counter;            /* last level: the count this term adds to */
+    int8_t reserved[3];
+} khz_term;
+typedef struct khz_level {
+    khz_term term;
+    int8_t has_cached;
+    int8_t finalized;
+    int8_t reserved[2];
+    khz_set_expr cached;
+} khz_level;
+typedef struct khz_pattern_schedule {
+    int8_t k;          /* pattern size, 3 .. 5 (MAX_PATTERN_SIZE, engine.h:23) */
+    int8_t num_terms;  /* counting terms of the last level, 1 or 2 */
+    int8_t reserved[2];
+    khz_level levels[5]; /* levels[1 .. k-2] are used */
+    khz_term last[2];
+} khz_pattern_schedule;
+typedef struct khz_app_desc {
+    int32_t num_runs;      /* patterns run one after another, each from every start vertex (1..6) */
+    int32_t num_counts;    /* counters (1..6) */
+    uint32_t multiplicity[KHZ_MAX_COUNTS]; /* raw counter / multiplicity = the reported count */
+    khz_pattern_schedule runs[6];
+} khz_app_desc;
+/* Validates the schedule and returns an app id (>= KHZ_NUM_APPS) usable everywhere a khz_app_id
+ * is, process-wide; such apps run on the DFS engine.  KHZ_ERR_ARG names the first invalid field. */
+khz_status khz_app_register(const khz_app_desc *desc, int32_t *app_id);
+
 /* ---- batched counting (many graphs / apps in one persistent launch) --------------- */
 typedef struct khz_job {
     khz_graph graph;
@@ -245,6 +307,10 @@ khz_status khz_server_wait(khz_server *server, khz_ticket ticket, uint64_t *coun
                            double *latency_ms, double timeout_ms);
 khz_status khz_server_stats_get(khz_server *server, khz_server_stats *stats);
 khz_status khz_server_reset_stats(khz_server *server);
+/* Withdraws a query that has not been admitted yet: its ticket then reports KHZ_ERR_CANCELLED.
+ * KHZ_ERR_BUSY if it already runs or has finished (its result stays available), KHZ_ERR_NOT_FOUND
+ * for an unknown or consumed ticket. */
+khz_status khz_server_cancel(khz_server *server, khz_ticket ticket);
 /* Finishes every submitted query, then releases the server. */
 khz_status khz_server_destroy(khz_server *server);
 

@@ -11,6 +11,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <initializer_list>
 #include <vector>
 
 #include "khz.h"
@@ -43,6 +44,96 @@ class Aggregator {
   private:
     T value_ = 0;
 };
+
+// Builder for a schedule an app brings itself (khz_app_register): the apply() levels written as
+// data.  Sets: N(i) = N(v_i), Set(2|3) = the set materialised by level 2 / 3, Cached() = the level's
+// cached set; .And(b) / .Sub(b) = intersect_with / subtracted_by N(v_b) (vertex_set.cc:20-86).
+struct SetExpr {
+    khz_set_expr e;
+    static SetExpr N(int i) { return SetExpr{{KHZ_BASE_NBR, (int8_t)i, {KHZ_OP_NONE, KHZ_OP_NONE}, {0, 0}}}; }
+    static SetExpr Set(int s) { return SetExpr{{KHZ_BASE_SET, (int8_t)s, {KHZ_OP_NONE, KHZ_OP_NONE}, {0, 0}}}; }
+    static SetExpr Cached() { return Set(4); }
+    SetExpr And(int b) const { return with(KHZ_OP_AND, b); }
+    SetExpr Sub(int b) const { return with(KHZ_OP_SUB, b); }
+
+  private:
+    SetExpr with(int op, int b) const {
+        SetExpr r = *this;
+        const int k = r.e.op[0] == KHZ_OP_NONE ? 0 : 1;
+        r.e.op[k] = (int8_t)op;
+        r.e.op_arg[k] = (int8_t)b;
+        return r;
+    }
+};
+
+// A candidate set with the generated code's filters: Above({a, ...}) keeps x > v_a for each a,
+// Except({a, ...}) keeps x != v_a; for a counting term, Into(c) names its counter and
+// OnlyIf(lo, hi) evaluates it only when v_lo < v_hi.
+struct Term {
+    khz_term t{};
+    explicit Term(SetExpr s) {
+        t.set = s.e;
+        t.guard_lo = t.guard_hi = -1;
+    }
+    Term &Above(std::initializer_list<int> vs) {
+        for (int a : vs) t.gt_mask |= (uint8_t)(1u << a);
+        return *this;
+    }
+    Term &Except(std::initializer_list<int> vs) {
+        for (int a : vs) t.ne_mask |= (uint8_t)(1u << a);
+        return *this;
+    }
+    Term &Into(int counter) {
+        t.counter = (int8_t)counter;
+        return *this;
+    }
+    Term &OnlyIf(int lo, int hi) {
+        t.guard_lo = (int8_t)lo;
+        t.guard_hi = (int8_t)hi;
+        return *this;
+    }
+};
+
+class Schedule {
+  public:
+    explicit Schedule(int k) { s_.k = (int8_t)k; }
+    // the next enumerating level (levels 1 .. k-2, in order); `cached` is computed on entry
+    Schedule &Level(const Term &t, bool finalized = false) { return add(t, nullptr, finalized); }
+    Schedule &Level(const Term &t, const SetExpr &cached, bool finalized = false) { return add(t, &cached, finalized); }
+    Schedule &Count(const Term &t) {
+        if (s_.num_terms < 2) s_.last[s_.num_terms++] = t.t;
+        return *this;
+    }
+    const khz_pattern_schedule &get() const { return s_; }
+
+  private:
+    Schedule &add(const Term &t, const SetExpr *cached, bool finalized) {
+        if (next_ < 5) {
+            khz_level &l = s_.levels[next_++];
+            l.term = t.t;
+            l.finalized = finalized ? 1 : 0;
+            if (cached) {
+                l.has_cached = 1;
+                l.cached = cached->e;
+            }
+        }
+        return *this;
+    }
+    khz_pattern_schedule s_{};
+    int next_ = 1;
+};
+
+// Registers an app of one or more schedules run one after another; returns its app id.
+inline khz_app_id register_app(const std::vector<Schedule> &runs, const std::vector<uint32_t> &multiplicities) {
+    khz_app_desc d{};
+    d.num_runs = (int32_t)runs.size();
+    d.num_counts = (int32_t)multiplicities.size();
+    for (size_t i = 0; i < multiplicities.size() && i < KHZ_MAX_COUNTS; ++i) d.multiplicity[i] = multiplicities[i];
+    for (size_t r = 0; r < runs.size() && r < 6; ++r) d.runs[r] = runs[r].get();
+    int32_t id = 0;
+    check(khz_app_register(&d, &id));
+    return (khz_app_id)id;
+}
 
 class DistributedApplication {
   public:

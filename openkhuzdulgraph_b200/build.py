@@ -35,7 +35,8 @@ def _newer(target, deps):
 
 def build(verbose=False, ptxas_verbose=False):
     os.makedirs(OBJ, exist_ok=True)
-    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    headers = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h")) +
+               glob.glob(os.path.join(ROOT, "include", "*.cuh")))
     objs, cmds = [], []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")

@@ -25,7 +25,7 @@
 #include <cuda_runtime.h>
 
 #include "khz_internal.cuh"
-#include "setops.cuh"
+#include "khz_setops.cuh"
 
 namespace khz {
 

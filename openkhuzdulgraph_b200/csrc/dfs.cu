@@ -7,7 +7,7 @@
 // matched vertices live in registers, every materialised prefix ("cached object",
 // engine.h:592-613) lives in the warp's private slot of a global scratch arena (L2
 // resident for the common small sets), and every set operation is warp-cooperative
-// (setops.cuh).  Work distribution replaces WorkloadDistributer (engine.cc:1457-1496):
+// (include/khz_setops.cuh).  Work distribution replaces WorkloadDistributer (engine.cc:1457-1496):
 // a unit is one level-1 candidate, i.e. one CSR entry (v0, adj[e]); warps grab
 // contiguous chunks of units from one atomic counter, so hub start vertices are split
 // across many warps.  Per-job counters replace Aggregator<EdgeId> (engine.h:615-673):
@@ -17,7 +17,7 @@
 #include <algorithm>
 
 #include "khz_internal.cuh"
-#include "setops.cuh"
+#include "khz_setops.cuh"
 
 namespace khz {
 
@@ -182,9 +182,9 @@ __device__ void dfs_level(WarpCtx &c) {
         if (lv.t.set.op[0] == OP_NONE) {
             base_of(c, lv.t.set, S, ns);
         } else {
-            // bounded materialisation: level sets are only ever re-read above their own lower
-            // bound (every later use filters by a larger matched vertex), see the plan tables
-            c.slot_len[L] = materialise<STATS>(c, lv.t.set, L, f, !STATS);
+            // bounded materialisation where the plan allows it: level sets then are only ever
+            // re-read above their own lower bound (every later use filters by a larger matched vertex)
+            c.slot_len[L] = materialise<STATS>(c, lv.t.set, L, f, !STATS && p.bounded_sets);
             __syncwarp();
             S = c.slot(L);
             ns = c.slot_len[L];

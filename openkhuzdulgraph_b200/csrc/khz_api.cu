@@ -11,12 +11,13 @@
 #include <memory>
 #include <thread>
 #include <mutex>
+#include <atomic>
 #include <string>
 #include <unordered_map>
 #include <vector>
 
 #include "khz_internal.cuh"
-#include "setops.cuh"
+#include "khz_setops.cuh"
 
 namespace khz {
 
@@ -168,12 +169,17 @@ struct BatchPlan {
     std::vector<khz_graph> graphs;       // graphs (and oriented views) whose pointers the plan holds
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    std::atomic<uint64_t> *direct_bytes = nullptr;  // the context's count of cudaMalloc'd bytes (mem not pooled)
     ~BatchPlan() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (mem) {
-            if (pool_mem) cudaFreeAsync(mem, pool_stream);
-            else cudaFree(mem);
+            if (pool_mem) {
+                cudaFreeAsync(mem, pool_stream);
+            } else {
+                cudaFree(mem);
+                if (direct_bytes) *direct_bytes -= mem_bytes;
+            }
         }
         if (h_final && own_pinned) cudaFreeHost(h_final);
     }
@@ -192,6 +198,7 @@ struct khz_ctx {
     uint32_t *shared_slots = nullptr;
     uint64_t shared_slot_words = 0;
     uint64_t *h_pinned = nullptr;  // kRowWords + 1 words
+    std::atomic<uint64_t> direct_bytes{0};  // device bytes held outside the pool (cudaMalloc)
     std::mutex mu;
 };
 
@@ -223,6 +230,7 @@ struct ServeResult {
     uint64_t counts[KHZ_MAX_COUNTS] = {};
     uint64_t num_ext = 0;
     double latency_ms = 0;
+    std::string error;  // why the query failed (the scheduler thread's error text)
 };
 
 struct ServeSlot {
@@ -257,6 +265,24 @@ struct khz_server {
 
 namespace {
 
+// Device bytes the context holds: its pool (graphs, pooled scratch) and its direct allocations.
+uint64_t ctx_device_bytes(khz_ctx *ctx) {
+    unsigned long long used = 0;  // the attribute's value is a 64-bit unsigned integer
+    if (ctx->pool) cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    return (uint64_t)used + ctx->direct_bytes.load();
+}
+
+// khz_config.device_mem_limit_mib: true (and the error set) when `more` bytes would pass the cap
+bool over_mem_limit(khz_ctx *ctx, uint64_t more, const char *what) {
+    const int32_t mib = ctx->cfg.device_mem_limit_mib;
+    if (mib <= 0) return false;
+    const uint64_t held = ctx_device_bytes(ctx), cap = (uint64_t)mib << 20;
+    if (held + more <= cap) return false;
+    set_error("%s: %llu more bytes would pass the context's device memory limit (%llu of %llu bytes held)", what,
+              (unsigned long long)more, (unsigned long long)held, (unsigned long long)cap);
+    return true;
+}
+
 khz_status check_ctx(khz_ctx *ctx) {
     if (!ctx) {
         set_error("null context");
@@ -279,6 +305,18 @@ khz_graph add_graph(khz_ctx *ctx, const Graph &g) {
     ctx->graphs.push_back(g);
     ctx->live.push_back(true);
     return (khz_graph)ctx->graphs.size();
+}
+
+// a graph built by an API call: registered, or released again (KHZ_ERR_OOM) when holding it passes
+// the context's device memory limit (the caller's AllocScope is still active, so the release
+// goes back to the pool)
+khz_status register_graph(khz_ctx *ctx, Graph &g, khz_graph *out) {
+    if (over_mem_limit(ctx, 0, "graph")) {
+        free_graph_memory(&g);
+        return KHZ_ERR_OOM;
+    }
+    *out = add_graph(ctx, g);
+    return KHZ_OK;
 }
 
 // oriented view of g (g itself when oriented; else a cached orientation)
@@ -339,7 +377,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         return KHZ_ERR_ARG;
     }
     for (int i = 0; i < n; ++i) {
-        if (jobs[i].app < 0 || jobs[i].app >= KHZ_NUM_APPS) {
+        if (!app_known(jobs[i].app)) {
             set_error("invalid app id %d", jobs[i].app);
             return KHZ_ERR_ARG;
         }
@@ -458,6 +496,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     if (!mjobs.empty()) bytes += Arena::round(sizeof(MJob) * mjobs.size());
     if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
     P->slot_words = P->has_dfs ? dfs_slot_words(ctx->cfg.dfs_warps_per_sm, slot_cap) : 0;
+    if (over_mem_limit(ctx, bytes, "counting launch scratch")) return KHZ_ERR_OOM;
     cudaError_t e;
     if (opts & kPlanPoolMem) {
         e = cudaMallocFromPoolAsync(&P->mem, bytes, ctx->pool, s);
@@ -467,6 +506,10 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         }
     } else {
         e = cudaMalloc(&P->mem, bytes);
+        if (e == cudaSuccess) {
+            ctx->direct_bytes += bytes;
+            P->direct_bytes = &ctx->direct_bytes;
+        }
     }
     P->mem_bytes = bytes;
     if (e != cudaSuccess) {
@@ -619,10 +662,15 @@ khz_status ensure_shared(khz_ctx *ctx, uint64_t words) {
         }
     }
     if (words > ctx->shared_slot_words) {
-        if (ctx->shared_slots) cudaFree(ctx->shared_slots);  // waits for work still using it
+        if (ctx->shared_slots) {
+            cudaFree(ctx->shared_slots);  // waits for work still using it
+            ctx->direct_bytes -= sizeof(uint32_t) * ctx->shared_slot_words;
+        }
         ctx->shared_slots = nullptr;
         ctx->shared_slot_words = 0;
+        if (over_mem_limit(ctx, sizeof(uint32_t) * words, "DFS scratch")) return KHZ_ERR_OOM;
         cudaError_t e = cudaMalloc(&ctx->shared_slots, sizeof(uint32_t) * words);
+        if (e == cudaSuccess) ctx->direct_bytes += sizeof(uint32_t) * words;
         if (e != cudaSuccess) {
             cudaGetLastError();
             ctx->shared_slots = nullptr;
@@ -642,7 +690,7 @@ double now_s() {
 // HBM scratch one query needs while it runs: DFS slots sized by the graph's largest degree, or
 // the bitmap engine's start-vertex lists; the CSR itself is resident and not counted
 khz_status serve_footprint(khz_server *sv, khz_graph h, int app, uint64_t *bytes) {
-    const uint64_t key = ((uint64_t)h << 8) | (uint64_t)app;
+    const uint64_t key = ((uint64_t)h << 20) | (uint64_t)app;
     std::lock_guard<std::mutex> fl(sv->fp_mu);  // lock order: fp_mu, then ctx->mu; never sv->mu here
     auto it = sv->footprints.find(key);
     if (it != sv->footprints.end()) {
@@ -760,10 +808,12 @@ void serve_dispatch(khz_server *sv) {
             if (e != cudaSuccess) st = cuda_fail(e, "serving dispatch");
         }
         if (st != KHZ_OK) {
+            const std::string why = khz_last_error_string();
             std::lock_guard<std::mutex> lk(sv->mu);
             for (auto &r : take) {
                 ServeResult &res = sv->results[r.id];
                 res.status = st;
+                res.error = why;
                 res.done = true;
             }
             sv->in_use -= fp;
@@ -940,8 +990,7 @@ khz_status khz_graph_from_edges(khz_ctx *ctx, const uint32_t *pairs, uint64_t m,
         if (st) return st;
         g = o;
     }
-    *out = add_graph(ctx, g);
-    return KHZ_OK;
+    return register_graph(ctx, g, out);
 }
 
 khz_status khz_graph_load_dgraph(khz_ctx *ctx, const char *path, uint32_t flags, khz_graph *out) {
@@ -1026,8 +1075,7 @@ khz_status khz_graph_orient(khz_ctx *ctx, khz_graph in, khz_graph *out, void *st
     AllocScope scope(ctx->pool, (cudaStream_t)stream);
     st = orient_graph(*g, &o, (cudaStream_t)stream);
     if (st) return st;
-    *out = add_graph(ctx, o);
-    return KHZ_OK;
+    return register_graph(ctx, o, out);
 }
 
 khz_status khz_graph_generate_rmat(khz_ctx *ctx, int scale, int edge_factor, double a, double b, double c,
@@ -1054,8 +1102,7 @@ khz_status khz_graph_generate_rmat(khz_ctx *ctx, int scale, int edge_factor, dou
         if (st) return st;
         g = o;
     }
-    *out = add_graph(ctx, g);
-    return KHZ_OK;
+    return register_graph(ctx, g, out);
 }
 
 khz_status khz_graph_info_get(khz_ctx *ctx, khz_graph h, khz_graph_info *info) {
@@ -1231,12 +1278,12 @@ khz_status khz_graph_free(khz_ctx *ctx, khz_graph h) {
 }
 
 int khz_app_num_counts(khz_app_id app) {
-    if (app < 0 || app >= KHZ_NUM_APPS) return 0;
+    if (!app_known(app)) return 0;
     return app_def(app).num_counts;
 }
 
 int khz_app_multiplicity(khz_app_id app, int pattern) {
-    if (app < 0 || app >= KHZ_NUM_APPS) return 0;
+    if (!app_known(app)) return 0;
     const AppDef &d = app_def(app);
     if (pattern < 0 || pattern >= d.num_counts) return 0;
     return (int)d.mult[pattern];
@@ -1274,7 +1321,7 @@ khz_status count_one(khz_ctx *ctx, khz_graph g, khz_app_id app, int64_t start_la
         set_error("null counts");
         return KHZ_ERR_ARG;
     }
-    if (app < 0 || app >= KHZ_NUM_APPS) {
+    if (!app_known(app)) {
         set_error("invalid app id %d", (int)app);
         return KHZ_ERR_ARG;
     }
@@ -1448,7 +1495,7 @@ khz_status khz_server_submit(khz_server *sv, khz_graph g, khz_app_id app, khz_ti
         set_error("null argument");
         return KHZ_ERR_ARG;
     }
-    if (app < 0 || app >= KHZ_NUM_APPS) {
+    if (!app_known(app)) {
         set_error("invalid app id %d", (int)app);
         return KHZ_ERR_ARG;
     }
@@ -1506,8 +1553,12 @@ khz_status khz_server_wait(khz_server *sv, khz_ticket ticket, uint64_t *counts, 
     }
     ServeResult r = sv->results[ticket];
     sv->results.erase(ticket);
+    if (r.status == KHZ_ERR_CANCELLED) {
+        set_error("ticket %llu was cancelled before it ran", (unsigned long long)ticket);
+        return r.status;
+    }
     if (r.status != KHZ_OK) {
-        set_error("query failed (status %d)", (int)r.status);
+        set_error("query failed (status %d): %s", (int)r.status, r.error.c_str());
         return r.status;
     }
     if (counts)
@@ -1547,6 +1598,32 @@ khz_status khz_server_reset_stats(khz_server *sv) {
     sv->batches = 0;
     sv->max_in_flight = sv->in_use;
     sv->t_first = -1;
+    return KHZ_OK;
+}
+
+khz_status khz_server_cancel(khz_server *sv, khz_ticket ticket) {
+    if (!sv) {
+        set_error("null server");
+        return KHZ_ERR_ARG;
+    }
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        auto it = sv->results.find(ticket);
+        if (it == sv->results.end()) {
+            set_error("unknown ticket %llu", (unsigned long long)ticket);
+            return KHZ_ERR_NOT_FOUND;
+        }
+        auto p = std::find_if(sv->pending.begin(), sv->pending.end(),
+                              [&](const ServeRequest &r) { return r.id == ticket; });
+        if (p == sv->pending.end()) {
+            set_error("ticket %llu is already admitted or finished", (unsigned long long)ticket);
+            return KHZ_ERR_BUSY;
+        }
+        sv->pending.erase(p);
+        it->second.status = KHZ_ERR_CANCELLED;
+        it->second.done = true;
+    }
+    sv->cv_done.notify_all();
     return KHZ_OK;
 }
 

@@ -52,7 +52,9 @@ struct Level {
 struct Plan {
     int8_t k;          // pattern size; levels 1..k-2 enumerate, level k-1 counts
     int8_t num_terms;  // counting terms at level k-1 (1 or 2)
-    int8_t pad[2];
+    int8_t bounded_sets;  // 1: every later use of a level's set filters above that level's own lower
+                          // bound, so level sets may be materialised without their members below it
+    int8_t pad;
     Level lv[kMaxK];   // lv[1..k-2]; lv[1] must enumerate N(v0) (the DFS unit is one CSR entry)
     Term last[2];
 };
@@ -69,6 +71,7 @@ struct AppDef {
 };
 
 const AppDef &app_def(int app);
+bool app_known(int app);  // a built-in app or one registered with khz_app_register
 
 // ---------------------------------------------------------------------------------
 // Device graph

@@ -17,7 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "khz_internal.cuh"
-#include "setops.cuh"
+#include "khz_setops.cuh"
 
 namespace khz {
 namespace {

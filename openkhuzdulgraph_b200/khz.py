@@ -38,7 +38,7 @@ SETOP = {"intersect": 0, "subtract": 1, "intersect_count": 2, "bounded_intersect
 
 STATUS = {0: "KHZ_OK", 1: "KHZ_ERR_ARG", 2: "KHZ_ERR_OOM", 3: "KHZ_ERR_OVERFLOW", 4: "KHZ_ERR_TIMEOUT",
           5: "KHZ_ERR_CUDA", 6: "KHZ_ERR_FORMAT", 7: "KHZ_ERR_BUSY", 8: "KHZ_ERR_NOT_FOUND",
-          9: "KHZ_ERR_MULTIPLICITY"}
+          9: "KHZ_ERR_MULTIPLICITY", 10: "KHZ_ERR_CANCELLED"}
 
 # every entry point include/khz.h declares
 EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_get_config",
@@ -49,7 +49,8 @@ EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_g
            "khz_app_multiplicity", "khz_count_batch", "khz_set_op_batch", "khz_count_noalloc",
            "khz_batch_create", "khz_batch_launch", "khz_batch_wait", "khz_batch_destroy",
            "khz_server_create", "khz_server_submit", "khz_server_wait", "khz_server_stats_get",
-           "khz_server_reset_stats", "khz_server_destroy", "khz_autotune"]
+           "khz_server_reset_stats", "khz_server_cancel", "khz_server_destroy", "khz_autotune",
+           "khz_app_register"]
 
 
 class KhzError(RuntimeError):
@@ -85,7 +86,8 @@ class Config(ctypes.Structure):
     _fields_ = [("engine", ctypes.c_int32), ("want_algo_bytes", ctypes.c_int32),
                 ("dfs_warps_per_sm", ctypes.c_int32), ("dfs_chunk", ctypes.c_int32),
                 ("bitmap_warp_max", ctypes.c_int32), ("bitmap_block_warps", ctypes.c_int32),
-                ("bitmap_hub_rows", ctypes.c_int32), ("reserved", ctypes.c_int32 * 9)]
+                ("bitmap_hub_rows", ctypes.c_int32), ("device_mem_limit_mib", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 8)]
 
 
 class ServerStats(ctypes.Structure):
@@ -104,6 +106,116 @@ class TuneReport(ctypes.Structure):
 
 class Job(ctypes.Structure):
     _fields_ = [("graph", ctypes.c_uint32), ("app", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+# ---- schedules an app brings itself (khz_app_register; the apply() levels as data) -------------
+class SetExpr(ctypes.Structure):
+    _fields_ = [("base_kind", ctypes.c_int8), ("base_arg", ctypes.c_int8), ("op", ctypes.c_int8 * 2),
+                ("op_arg", ctypes.c_int8 * 2)]
+
+
+class Term(ctypes.Structure):
+    _fields_ = [("set", SetExpr), ("gt_mask", ctypes.c_uint8), ("ne_mask", ctypes.c_uint8),
+                ("guard_lo", ctypes.c_int8), ("guard_hi", ctypes.c_int8), ("counter", ctypes.c_int8),
+                ("reserved", ctypes.c_int8 * 3)]
+
+
+class Level(ctypes.Structure):
+    _fields_ = [("term", Term), ("has_cached", ctypes.c_int8), ("finalized", ctypes.c_int8),
+                ("reserved", ctypes.c_int8 * 2), ("cached", SetExpr)]
+
+
+class PatternSchedule(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_int8), ("num_terms", ctypes.c_int8), ("reserved", ctypes.c_int8 * 2),
+                ("levels", Level * 5), ("last", Term * 2)]
+
+
+class AppDesc(ctypes.Structure):
+    _fields_ = [("num_runs", ctypes.c_int32), ("num_counts", ctypes.c_int32),
+                ("multiplicity", ctypes.c_uint32 * 6), ("runs", PatternSchedule * 6)]
+
+
+BASE_NBR, BASE_SET = 0, 1
+OP_NONE, OP_AND, OP_SUB = 0, 1, 2
+
+
+def N(i):
+    """N(v_i): the neighbour list of matched vertex i."""
+    return (BASE_NBR, i, [])
+
+
+def S(s):
+    """A set materialised earlier: 2 or 3 = level 2 / 3's set, 4 = the cached set."""
+    return (BASE_SET, s, [])
+
+
+def AND(e, b):
+    """e.intersect_with(N(v_b))"""
+    return (e[0], e[1], e[2] + [(OP_AND, b)])
+
+
+def SUB(e, b):
+    """e.subtracted_by(N(v_b))"""
+    return (e[0], e[1], e[2] + [(OP_SUB, b)])
+
+
+def _mask(vs):
+    m = 0
+    for v in vs:
+        m |= 1 << v
+    return m
+
+
+def _set_expr(dst, e):
+    dst.base_kind, dst.base_arg = e[0], e[1]
+    if len(e[2]) > 2:
+        raise ValueError("at most two operations per set")
+    for k, (o, b) in enumerate(e[2]):
+        dst.op[k], dst.op_arg[k] = o, b
+
+
+def _term(dst, t):
+    e, gt, ne, counter, guard = t
+    _set_expr(dst.set, e)
+    dst.gt_mask, dst.ne_mask, dst.counter = _mask(gt), _mask(ne), counter
+    dst.guard_lo, dst.guard_hi = guard if guard else (-1, -1)
+
+
+def term(e, gt=(), ne=(), counter=0, guard=None):
+    """A level's candidate set with its filters: keep x > v_a (a in gt) and x != v_a (a in ne);
+    at the last level, adds to `counter`, only when v[guard[0]] < v[guard[1]] if a guard is given."""
+    return (e, tuple(gt), tuple(ne), counter, guard)
+
+
+def level(t, cached=None, finalized=False):
+    return (t, cached, finalized)
+
+
+def schedule(k, levels, last):
+    """k: pattern size; levels: the enumerating levels 1 .. k-2; last: 1 or 2 counting terms."""
+    return (k, list(levels), list(last))
+
+
+def register_app(runs, multiplicities):
+    """Registers an app made of `runs` (schedules run one after another) -> its app id."""
+    d = AppDesc()
+    d.num_runs, d.num_counts = len(runs), len(multiplicities)
+    for c, m in enumerate(multiplicities):
+        d.multiplicity[c] = m
+    for r, (k, levels, last) in enumerate(runs):
+        ps = d.runs[r]
+        ps.k, ps.num_terms = k, len(last)
+        for li, (t, cached, fin) in enumerate(levels, start=1):
+            _term(ps.levels[li].term, t)
+            ps.levels[li].finalized = 1 if fin else 0
+            if cached is not None:
+                ps.levels[li].has_cached = 1
+                _set_expr(ps.levels[li].cached, cached)
+        for ti, t in enumerate(last):
+            _term(ps.last[ti], t)
+    app = ctypes.c_int32(0)
+    _check(lib().khz_app_register(ctypes.byref(d), ctypes.byref(app)))
+    return app.value
 
 
 _lib = None
@@ -152,8 +264,10 @@ def lib():
             "khz_server_wait": (i32, [vp, u64, P(u64), P(u64), P(ctypes.c_double), ctypes.c_double]),
             "khz_server_stats_get": (i32, [vp, P(ServerStats)]),
             "khz_server_reset_stats": (i32, [vp]),
+            "khz_server_cancel": (i32, [vp, u64]),
             "khz_server_destroy": (i32, [vp]),
             "khz_autotune": (i32, [vp, P(Job), i32, i32, P(TuneReport)]),
+            "khz_app_register": (i32, [P(AppDesc), P(ctypes.c_int32)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -392,6 +506,14 @@ class Server:
 
     def reset_stats(self):
         _check(lib().khz_server_reset_stats(self.ptr))
+
+    def cancel(self, ticket):
+        """Withdraws a query not yet admitted -> True; False if it already runs or has finished."""
+        rc = lib().khz_server_cancel(self.ptr, ticket)
+        if rc == 7:  # KHZ_ERR_BUSY
+            return False
+        _check(rc)
+        return True
 
     def close(self):
         if self.ptr:

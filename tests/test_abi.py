@@ -56,7 +56,8 @@ def test_config_layout_is_fixed():
     """khz_config keeps its size when fields are taken from the reserved words (64 bytes)."""
     import ctypes
     assert ctypes.sizeof(khz.Config) == 64
-    assert khz.Config.bitmap_hub_rows.offset == 24 and khz.Config.reserved.offset == 28
+    assert khz.Config.bitmap_hub_rows.offset == 24 and khz.Config.device_mem_limit_mib.offset == 28
+    assert khz.Config.reserved.offset == 32
 
 
 def test_graph_info_layout():

@@ -66,3 +66,112 @@ def test_ticket_errors(khz_ctx, resident):
         assert e.value.status == 1
     finally:
         sv.close()
+
+
+# ---- failures made on the host (no device fault is ever provoked) -------------------------------
+@pytest.fixture(scope="module")
+def heavy(khz_ctx):
+    """A graph whose house count on the DFS engine takes milliseconds, so queued queries wait."""
+    canon, n = orc.rmat(13, 16, seed=9)
+    g = khz_ctx.graph_from_edges(orc.symmetrize(canon), n)
+    alone = khz_ctx.count(g, "kgraphpi_house")
+    yield g, alone
+    g.free()
+
+
+def test_allocation_failure_reaches_tickets_without_stalling(khz_ctx, resident):
+    """With the context's device memory capped below what it already holds, every launch's scratch
+    allocation fails on the host side of the scheduler: each ticket reports KHZ_ERR_OOM promptly and
+    the server keeps serving once the cap is lifted."""
+    from openkhuzdulgraph_b200 import khz
+    graphs, alone = resident
+    sv = khz.Server(khz_ctx, slots=2, max_batch=4)
+    try:
+        khz_ctx.set_config(device_mem_limit_mib=1)
+        tickets = [(sv.submit(graphs[i % len(graphs)], app), i % len(graphs), app)
+                   for i, app in enumerate(APPS * 3)]
+        for t, _, app in tickets:
+            with pytest.raises(khz.KhzError) as e:
+                sv.wait(t, app, timeout_ms=20000.0)
+            assert e.value.status == 2 and "memory limit" in str(e.value)
+        khz_ctx.set_config(device_mem_limit_mib=0)
+        for i, app in [(0, "kautomine_four_clique"), (3, "kgraphpi_house")]:
+            counts, ext, _ = sv.wait(sv.submit(graphs[i], app), app, timeout_ms=20000.0)
+            exp, st = alone[(i, app)]
+            assert counts == exp and ext == st.num_extensions
+    finally:
+        khz_ctx.set_config(device_mem_limit_mib=0)
+        sv.close()
+
+
+def test_memory_limit_rejects_graphs_and_counts(khz_ctx):
+    from openkhuzdulgraph_b200 import khz
+    canon, n = orc.rmat(10, 8, seed=4)
+    sym = orc.symmetrize(canon)
+    g = khz_ctx.graph_from_edges(sym, n)
+    try:
+        khz_ctx.set_config(device_mem_limit_mib=1)
+        with pytest.raises(khz.KhzError) as e:
+            khz_ctx.graph_from_edges(sym, n)
+        assert e.value.status == 2
+        with pytest.raises(khz.KhzError) as e:
+            khz_ctx.count(g, "kautomine_four_clique")
+        assert e.value.status == 2
+        khz_ctx.set_config(device_mem_limit_mib=0)
+        off, adj = orc.csr(sym, n)
+        assert khz_ctx.count(g, "kautomine_four_clique")[0] == orc.count("kautomine_four_clique", off, adj)[0]
+    finally:
+        khz_ctx.set_config(device_mem_limit_mib=0)
+        g.free()
+
+
+def test_timed_out_wait_then_success(khz_ctx, heavy):
+    """A wait that runs out returns KHZ_ERR_TIMEOUT (KHZ_ERR_BUSY when only polling) and leaves the
+    ticket valid: a later wait returns the result."""
+    from openkhuzdulgraph_b200 import khz
+    g, (exp, st) = heavy
+    sv = khz.Server(khz_ctx, slots=1, max_batch=1)
+    try:
+        tickets = [sv.submit(g, "kgraphpi_house") for _ in range(24)]
+        last = tickets[-1]
+        with pytest.raises(khz.KhzError) as e:
+            sv.wait(last, "kgraphpi_house", timeout_ms=0.0)
+        assert e.value.status == 7
+        with pytest.raises(khz.KhzError) as e:
+            sv.wait(last, "kgraphpi_house", timeout_ms=0.5)
+        assert e.value.status == 4
+        for t in tickets:
+            counts, ext, _ = sv.wait(t, "kgraphpi_house", timeout_ms=120000.0)
+            assert counts == exp and ext == st.num_extensions
+    finally:
+        sv.close()
+
+
+def test_cancel_withdraws_pending_queries(khz_ctx, heavy):
+    from openkhuzdulgraph_b200 import khz
+    g, (exp, st) = heavy
+    sv = khz.Server(khz_ctx, slots=1, max_batch=1)
+    try:
+        tickets = [sv.submit(g, "kgraphpi_house") for _ in range(40)]
+        cancelled = {t for t in tickets[20:] if sv.cancel(t)}
+        assert cancelled  # the queue of 40 cannot have drained this fast
+        for t in tickets:
+            if t in cancelled:
+                with pytest.raises(khz.KhzError) as e:
+                    sv.wait(t, "kgraphpi_house", timeout_ms=1000.0)
+                assert e.value.status == 10
+            else:
+                counts, ext, _ = sv.wait(t, "kgraphpi_house", timeout_ms=120000.0)
+                assert counts == exp and ext == st.num_extensions
+        with pytest.raises(khz.KhzError) as e:  # consumed
+            sv.cancel(tickets[0])
+        assert e.value.status == 8
+        # one slot, one query per launch, admission in arrival order: once t2 is done, t is done too
+        t = sv.submit(g, "kgraphpi_house")
+        t2 = sv.submit(g, "kgraphpi_house")
+        sv.wait(t2, "kgraphpi_house", timeout_ms=120000.0)
+        assert sv.cancel(t) is False  # finished, not yet consumed: too late to cancel
+        counts, _, _ = sv.wait(t, "kgraphpi_house", timeout_ms=120000.0)
+        assert counts == exp
+    finally:
+        sv.close()

@@ -71,6 +71,8 @@ def test_restricted_matches_oracle_every_app(golden, labelled, khz_ctx, engine):
         for spec, g, off, adj, labels in labelled:
             for app in ALL_APPS:
                 for lab in sorted({0, golden["sample"]["rem"], mod - 1}):
+                    if lab >= g.info().num_labels:  # a graph of fewer vertices than the modulus
+                        continue
                     exp, ext, _ = orc.count_labeled(app, off, adj, labels, lab, threads=4)
                     raw, st = khz_ctx.count_restricted(g, app, lab)
                     assert raw == exp, (spec["name"], app, lab, engine)
@@ -114,10 +116,12 @@ def test_label_slices_partition_the_whole_count(khz_ctx):
     g = khz_ctx.graph_from_edges(sym, n)
     og = g.orient()
     nl = 5
-    for gg in (g, og):
+    # every app on the symmetric graph; the clique apps on the oriented one (the others count
+    # patterns of an undirected graph, whose multiplicities a DAG does not honour)
+    for gg, apps in ((g, ALL_APPS), (og, CLIQUES)):
         labels = (np.arange(n, dtype=np.uint64) * 40503 % nl).astype(np.uint32)
         gg.set_labels(labels)
-        for app in ALL_APPS:
+        for app in apps:
             whole, st = khz_ctx.count(gg, app)
             mult = _mults(khz, app)
             tot, ext = [0] * len(whole), 0
