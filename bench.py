@@ -450,42 +450,90 @@ def batch_workload(args):
     t_gen = time.time() - t0
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
-    # plain: one query at a time (first pass prepares and caches each launch)
-    ref, emb = [], 0
+    steps = max(3, args.steps)
+    # plain: one query at a time (first pass prepares and caches each launch, and builds the
+    # per-graph views the engines use: one-time work, not a query's cost)
+    ref, exts_ref, emb = [], [], 0
     for g, app in jobs:
         cnt, st = ctx.count(g, app, stream=sptr)
         ref.append(cnt)
+        exts_ref.append(st.num_extensions)
         emb += st.num_extensions + sum(cnt)
-    plain_ms = []
-    for _ in range(args.steps):
+
+    def plain_pass(sel):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        for (g, app), r in zip(jobs, ref):
+        for k in sel:
+            g, app = jobs[k]
             cnt, _ = ctx.count(g, app, stream=sptr)
-            assert cnt == r
+            assert cnt == ref[k]
         torch.cuda.synchronize()
-        plain_ms.append((time.perf_counter() - t1) * 1000)
+        return (time.perf_counter() - t1) * 1000
+
+    everything = list(range(len(jobs)))
+    by_app = {app: [k for k, (_, a2) in enumerate(jobs) if a2 == app] for app in BATCH_APPS}
     batch = khz.Batch(ctx, jobs, cuda_graph=True, stream=sptr)
     batch.launch(sptr)
     counts, exts = batch.wait(sptr)
-    assert counts == ref
-    batch_ms = []
-    for _ in range(args.steps):
+    assert counts == ref and exts == exts_ref
+
+    def batch_pass(b):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        batch.launch(sptr)
-        counts, _ = batch.wait(sptr)
-        batch_ms.append((time.perf_counter() - t1) * 1000)
-        assert counts == ref
+        b.launch(sptr)
+        cnts, _ = b.wait(sptr)
+        ms = (time.perf_counter() - t1) * 1000
+        return ms, cnts
+
+    # served: every query of the batch submitted at once to the continuous-batching server
+    sv = khz.Server(ctx, slots=args.slots, max_batch=args.max_batch)
+    for k in range(0, len(jobs), 997):  # warm the scheduler's per-(graph, app) footprint cache
+        sv.wait(sv.submit(*jobs[k]), jobs[k][1], timeout_ms=600000.0)
+
+    def serve_pass():
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        tickets = [sv.submit(g, app) for g, app in jobs]
+        for k, t in enumerate(tickets):
+            cnt, ext, _ = sv.wait(t, jobs[k][1], timeout_ms=600000.0)
+            assert cnt == ref[k] and ext == exts_ref[k]
+        return (time.perf_counter() - t1) * 1000
+
+    plain_ms, batch_ms, serve_ms = [], [], []
+    with ClockSampler(0) as clk:
+        for _ in range(steps):
+            plain_ms.append(plain_pass(everything))
+            ms, cnts = batch_pass(batch)
+            assert cnts == ref
+            batch_ms.append(ms)
+            serve_ms.append(serve_pass())
+    sv.close()
     batch.close()
-    p_ms, b_ms = statistics.median(plain_ms), statistics.median(batch_ms)
+    # per app: plain vs one batched launch sequence of that app's queries (median of `steps`)
+    per_app = {}
+    for app, sel in by_app.items():
+        if not sel:
+            continue
+        b = khz.Batch(ctx, [jobs[k] for k in sel], cuda_graph=True, stream=sptr)
+        b.launch(sptr)
+        b.wait(sptr)
+        pm = statistics.median(plain_pass(sel) for _ in range(steps))
+        bm = statistics.median(batch_pass(b)[0] for _ in range(steps))
+        b.close()
+        per_app[app] = {"queries": len(sel), "ms_plain": pm, "ms_batched": bm, "batched_over_plain": pm / bm}
+    p_ms, b_ms, s_ms = statistics.median(plain_ms), statistics.median(batch_ms), statistics.median(serve_ms)
     print(json.dumps({
         "metric": "embeddings/s (uneven batch of %d graphs)" % len(jobs), "unit": "embeddings/s",
-        "value": emb / (b_ms / 1000), "plain_value": emb / (p_ms / 1000), "batched_over_plain": p_ms / b_ms,
-        "ms_batched": b_ms, "ms_plain": p_ms, "embeddings": emb, "graphs": len(jobs), "csr_entries": edges,
-        "generation_s": t_gen, "steps": args.steps, "higher_is_better": True, "data": "synthetic (device R-MAT)",
+        "value": emb / (b_ms / 1000), "plain_value": emb / (p_ms / 1000), "served_value": emb / (s_ms / 1000),
+        "batched_over_plain": p_ms / b_ms, "served_over_plain": p_ms / s_ms,
+        "ms_batched": b_ms, "ms_plain": p_ms, "ms_served": s_ms,
+        "ms_steps": {"plain": plain_ms, "batched": batch_ms, "served": serve_ms}, "per_app": per_app,
+        "embeddings": emb, "graphs": len(jobs), "csr_entries": edges, "generation_s": t_gen, "steps": steps,
+        "slots": args.slots, "max_batch": args.max_batch, "clocks": clk.summary(), "higher_is_better": True,
+        "data": "synthetic (device R-MAT)",
         "config": {"workload": "uneven batch: n log-uniform [64, 200000], degree U[4, 40], "
-                               "apps %s" % BATCH_APPS}}), flush=True)
+                               "apps %s" % BATCH_APPS,
+                   "timing": "wall clock per pass (host calls included), median of %d" % steps}}), flush=True)
     ctx.close()
 
 
@@ -522,7 +570,7 @@ def serve_workload(args):
     sizes = [g.num_entries // 2 for g in graphs]
     t_gen = time.time() - t0
     # feasibility: per app, graphs in increasing size until one query alone exceeds the cap
-    feasible, alone = [], {}
+    feasible, alone, first_excluded = [], {}, {}
     for app in SERVE_APPS:  # load every kernel once
         ctx.count(graphs[0], app)
     for app in SERVE_APPS:
@@ -533,9 +581,13 @@ def serve_workload(args):
             dt = (time.perf_counter() - t1) * 1000
             alone[(gi, app)] = (cnt, st.num_extensions, dt)
             if dt > args.query_cap_ms:
+                first_excluded[app] = {"graph": gi, "undirected_edges": int(sizes[gi]), "ms_alone": dt,
+                                       "excluded_graphs": len(graphs) - gi}
                 break
             feasible.append((gi, app))
     rng = random.Random(11)
+    clk = ClockSampler(0)
+    clk.__enter__()
     sv = khz.Server(ctx, slots=args.slots, max_batch=args.max_batch)
     # warm: every feasible query once through the server
     for gi, app in feasible:
@@ -590,7 +642,9 @@ def serve_workload(args):
     for gi, app in qs:
         ctx.count(graphs[gi], app)
     plain_s = time.perf_counter() - t1
+    clk.__exit__(None, None, None)
     out = {"metric": "served queries/s and latency (continuous batching)", "unit": "queries/s",
+           "clocks": clk.summary(), "excluded": first_excluded,
            "value": len(qs) / served_s, "plain_value": len(qs) / plain_s, "served_over_plain": plain_s / served_s,
            "rates": rates_out, "graphs": len(graphs), "undirected_edges_total": int(sum(sizes)),
            "largest_graph_edges": int(max(sizes)), "feasible_queries": len(feasible),
@@ -601,6 +655,50 @@ def serve_workload(args):
                                   "(log-spaced), apps %s; a (graph, app) pair is served when that query alone "
                                   "takes <= query_cap_ms" % SERVE_APPS}}
     print(json.dumps(out), flush=True)
+    ctx.close()
+
+
+CONFIG_RUNS = [
+    # (label, scale, edge factor, oriented, apps): the triangle configuration is the ER graph
+    ("K: R-MAT s22 ef16, degree-oriented", 22, 16, True, ["kautomine_four_clique", "kgraphpi_four_clique",
+                                                       "kautomine_five_clique", "kgraphpi_five_clique"]),
+    ("M: R-MAT s20 ef24, symmetric", 20, 24, False, ["kautomine_triangle", "kautomine_three_motif",
+                                                    "kgraphpi_three_motif", "kgraphpi_four_cycle",
+                                                    "kgraphpi_tailed_triangle", "kautomine_four_motif"]),
+]
+
+
+def configs_workload(args):
+    """Every app of the full-size configurations, device time per count (median of the steps), with
+    the engine each app took; the house schedule on M is left out (only the DFS engine runs it, and
+    its work grows with the square of hub degrees)."""
+    import torch
+    from openkhuzdulgraph_b200 import khz
+    torch.cuda.set_device(0)
+    ctx = khz.Context(0)
+    a, b, c = RMAT_ABC
+    steps = max(3, args.steps)
+    out = []
+    with ClockSampler(0) as clk:
+        for label, scale, ef, oriented, apps in CONFIG_RUNS:
+            sym = ctx.generate_rmat(scale, ef, a, b, c, SEED)
+            g = sym.orient() if oriented else sym
+            if oriented:
+                sym.free()
+            for app in apps:
+                cnt, st = ctx.count(g, app)  # one-time work (views, prepared launch) first
+                ms = []
+                for _ in range(steps):
+                    c2, st = ctx.count(g, app)
+                    assert c2 == cnt
+                    ms.append(st.kernel_ms)
+                out.append({"config": label, "app": app, "counts": cnt, "num_extensions": st.num_extensions,
+                            "ms": statistics.median(ms), "engine": ["auto", "dfs", "bitmap", "wedge"][st.engine],
+                            "embeddings_per_s": (st.num_extensions + sum(cnt)) / (statistics.median(ms) / 1000)})
+                print(json.dumps(out[-1]), flush=True)
+            g.free()
+    print(json.dumps({"metric": "device time per count, full-size configurations", "runs": out,
+                      "clocks": clk.summary(), "steps": steps, "data": "synthetic (device R-MAT)"}), flush=True)
     ctx.close()
 
 
@@ -652,7 +750,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident steps only (profiling)")
-    ap.add_argument("--workload", default="clique4", choices=["clique4", "batch", "serve"],
+    ap.add_argument("--workload", default="clique4", choices=["clique4", "batch", "serve", "configs"],
                     help="clique4: the bench line; batch: the uneven multi-graph batch; serve: Poisson serving")
     ap.add_argument("--rates", type=float, nargs="+", default=[100, 500, 1000, 2000, 5000])
     ap.add_argument("--duration", type=float, default=2.0, help="seconds of arrivals per rate (serve)")
@@ -669,6 +767,9 @@ def main():
         return
     if args.workload == "serve":
         serve_workload(args)
+        return
+    if args.workload == "configs":
+        configs_workload(args)
         return
     if args.impl == "reference":
         # the reference arm is a CPU run on rank 0; other ranks exit without work

@@ -185,6 +185,36 @@ int khz_app_num_counts(khz_app_id app);
 /* mirrors the reference's `multiplicities[]` tables (kautomine/three_motif.cc:44) */
 int khz_app_multiplicity(khz_app_id app, int pattern);
 
+/* ---- frequent labelled subgraph mining (3-FSM) ------------------------------------ */
+/* The kautomine three_fsm app (kautomine/three_fsm.cc:53-800) on the device: single vertices,
+ * then edges, wedges, triangles, four-chains and three-stars of node labels, each level's candidate
+ * labellings generated from the previous levels' frequent patterns (three_fsm.cc:315-590); a
+ * pattern is frequent when its MNI support (for every pattern vertex the number of distinct graph
+ * vertices it maps to, the least of these: SharedMemoryPatternDomain::get_support,
+ * engine.h:384-401) reaches `threshold`.  The graph must carry node labels (at most 48, the
+ * reference's MAX_NUM_LABELS).  out->level[i] gives what the app prints per level (the number of
+ * frequent patterns and the support sum; level 0's sum covers every label, as setup() computes
+ * it).  patterns (may be NULL) receives up to `capacity` frequent canonical patterns in the order
+ * found; *num_patterns their total number. */
+typedef struct khz_fsm_level {
+    uint32_t num_candidates;
+    uint32_t num_frequent;
+    uint64_t support_sum;
+} khz_fsm_level;
+typedef struct khz_fsm_result {
+    khz_fsm_level level[6]; /* vertex, edge, wedge, triangle, four-chain, three-star */
+    double ms;              /* host wall time of the whole mining run */
+} khz_fsm_result;
+typedef struct khz_fsm_pattern {
+    uint32_t level;         /* index into khz_fsm_result.level */
+    uint32_t size;          /* pattern vertices */
+    uint32_t labels[4];     /* the canonical labelling, in the app's vertex order */
+    uint32_t support;
+    uint32_t reserved;
+} khz_fsm_pattern;
+khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz_fsm_result *out, khz_fsm_pattern *patterns,
+                   uint32_t capacity, uint32_t *num_patterns);
+
 /* ---- apps that bring their own schedule ------------------------------------------ */
 /* Replaces the ApplyFunction contract (engine.h:589) and the engine calls an apply() makes
  * (scatter / cached objects, engine.h:592-613, 846-859): an app describes its apply() levels as

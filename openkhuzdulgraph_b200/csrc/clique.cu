@@ -84,13 +84,16 @@ __host__ __device__ __forceinline__ uint64_t hub_row_offset(uint32_t h, uint32_t
 //                   32-bit words, read as W64 = ceil(d / 64) 64-bit words by the counting loops,
 //                   at a stride of S = 2 (W64 | 1) 32-bit words: odd in 64-bit words, so that
 //                   lanes reading the same word offset of different rows hit different banks
-//   rlo/rhi[d]      first / one-past-last non-zero 64-bit word of each row
+//   rext[d]         per row, its first (low 16 bits) and one-past-last (high 16 bits) non-zero
+//                   64-bit word: one shared load gives both
+__device__ __forceinline__ int ext_lo(uint32_t e) { return (int)(e & 0xffffu); }
+__device__ __forceinline__ int ext_hi(uint32_t e) { return (int)(e >> 16); }
 struct Local {
     uint32_t *c;
     uint32_t *hkey;
     uint16_t *hidx;
     uint32_t *rows;
-    uint16_t *rlo, *rhi;
+    uint32_t *rext;
     int d, W, W64, S, logt;
     __device__ __forceinline__ const uint64_t *row64(int i) const {
         return reinterpret_cast<const uint64_t *>(rows + (size_t)i * S);
@@ -237,19 +240,20 @@ __device__ __forceinline__ void row_extents(const Local &g, int tid, int nthr) {
                 hi = w + 1;
             }
         }
-        g.rlo[i] = (uint16_t)(hi == 0 ? g.W64 : lo);
-        g.rhi[i] = (uint16_t)hi;
+        g.rext[i] = (uint32_t)(hi == 0 ? g.W64 : lo) | ((uint32_t)hi << 16);
     }
 }
 
-template <int K, bool STATS>
+// WIDE: rows of many words (the large tiers), where the popcount loop runs two words per step
+template <int K, bool STATS, bool WIDE = false>
 __device__ __forceinline__ void process_item(const Local &g, int i, int j, const uint64_t *off, Acc &a) {
     const uint64_t *ri = g.row64(i);
     const uint64_t *rj = g.row64(j);
-    const int lo = max((int)g.rlo[i], (int)g.rlo[j]);
-    const int hi = min((int)g.rhi[i], (int)g.rhi[j]);
+    const uint32_t ei = g.rext[i], ej = g.rext[j];
+    const int lo = max(ext_lo(ei), ext_lo(ej));
+    const int hi = min(ext_hi(ei), ext_hi(ej));
     uint32_t s = 0;
-    {
+    if (!WIDE) {
         // the hot loop with 32-bit shared-window addresses stepped by one 64-bit word
         const uint32_t sb = (uint32_t)__cvta_generic_to_shared(g.rows);
         uint32_t ai = sb + (uint32_t)(i * g.S + 2 * lo) * 4u, aj = sb + (uint32_t)(j * g.S + 2 * lo) * 4u;
@@ -259,10 +263,33 @@ __device__ __forceinline__ void process_item(const Local &g, int i, int j, const
             asm("ld.shared.u64 %0, [%1];" : "=l"(y) : "r"(aj));
             s += __popcll(x & y);
         }
+    } else {
+        // two 64-bit words per step with independent sums (the popcounts of one step do not
+        // wait on each other)
+        const uint32_t sb = (uint32_t)__cvta_generic_to_shared(g.rows);
+        uint32_t ai = sb + (uint32_t)(i * g.S + 2 * lo) * 4u, aj = sb + (uint32_t)(j * g.S + 2 * lo) * 4u;
+        uint32_t s1 = 0;
+        int w = lo;
+        for (; w + 1 < hi; w += 2, ai += 16, aj += 16) {
+            uint64_t x0, y0, x1, y1;
+            asm("ld.shared.u64 %0, [%1];" : "=l"(x0) : "r"(ai));
+            asm("ld.shared.u64 %0, [%1];" : "=l"(y0) : "r"(aj));
+            asm("ld.shared.u64 %0, [%1+8];" : "=l"(x1) : "r"(ai));
+            asm("ld.shared.u64 %0, [%1+8];" : "=l"(y1) : "r"(aj));
+            s += __popcll(x0 & y0);
+            s1 += __popcll(x1 & y1);
+        }
+        if (w < hi) {
+            uint64_t x, y;
+            asm("ld.shared.u64 %0, [%1];" : "=l"(x) : "r"(ai));
+            asm("ld.shared.u64 %0, [%1];" : "=l"(y) : "r"(aj));
+            s += __popcll(x & y);
+        }
+        s += s1;
     }
     if (STATS) {
         uint32_t pi = 0;
-        for (int w = g.rlo[i]; w < g.rhi[i]; ++w) pi += __popcll(ri[w]);
+        for (int w = ext_lo(ei); w < ext_hi(ei); ++w) pi += __popcll(ri[w]);
         a.bytes += 4ull * ((uint64_t)pi + odeg(off, g.c[j]) + s);
     }
     if (K == 4) {
@@ -276,8 +303,9 @@ __device__ __forceinline__ void process_item(const Local &g, int i, int j, const
             const int l = (w1 << 6) + __ffsll((long long)m) - 1;
             m &= m - 1;
             const uint64_t *rl = g.row64(l);
-            const int lo3 = max(lo, (int)g.rlo[l]);
-            const int hi3 = min(hi, (int)g.rhi[l]);
+            const uint32_t el = g.rext[l];
+            const int lo3 = max(lo, ext_lo(el));
+            const int hi3 = min(hi, ext_hi(el));
             uint32_t t = 0;
             for (int w = lo3; w < hi3; ++w) t += __popcll(ri[w] & rj[w] & rl[w]);
             a.cnt += t;
@@ -360,7 +388,8 @@ __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_b
     uint32_t head = 0, tail = 0;  // ring positions (warp-uniform); pending items tail - head < 32
     for (int i = row_begin; i < g.d; i += row_step) {
         const uint64_t *ri = g.row64(i);
-        const int lo = g.rlo[i], hi = g.rhi[i];
+        const uint32_t ei = g.rext[i];
+        const int lo = ext_lo(ei), hi = ext_hi(ei);
         if (STATS && lane == 0) a.bytes += 4ull * ((uint64_t)g.d + odeg(off, g.c[i]));
         const uint32_t ibase = ((uint32_t)i << 16) + (uint32_t)lane;
         for (int w = lo; w < hi; ++w) {
@@ -380,8 +409,8 @@ __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_b
                 const uint32_t it = ring[(head + lane) & (kRing - 1)];
                 __syncwarp();
                 head += 32;
-                if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
-                else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+                if (KMAX == 4 || K == 4) process_item<4, STATS, true>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+                else process_item<5, STATS, true>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
             }
         }
     }
@@ -393,8 +422,8 @@ __device__ void count_rows(const Local &g, int K, const uint64_t *off, int row_b
     __syncwarp();
     if (K > 3 && (uint32_t)lane < tail - head) {
         const uint32_t it = ring[(head + lane) & (kRing - 1)];
-        if (KMAX == 4 || K == 4) process_item<4, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
-        else process_item<5, STATS>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+        if (KMAX == 4 || K == 4) process_item<4, STATS, true>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
+        else process_item<5, STATS, true>(g, (int)(it >> 16), (int)(it & 0xffffu), off, a);
     }
     __syncwarp();
 }
@@ -483,7 +512,7 @@ __global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restr
     __shared__ uint64_t s_rows[8][kWarpMax * S / 2];
     __shared__ uint32_t s_hkey[8][T];
     __shared__ uint16_t s_hidx[8][T];
-    __shared__ uint16_t s_rlo[8][kWarpMax], s_rhi[8][kWarpMax];
+    __shared__ uint32_t s_rext[8][kWarpMax];
     const unsigned lane = lane_id();
     const int wib = threadIdx.x >> 5;
     Local g;
@@ -491,8 +520,7 @@ __global__ void __launch_bounds__(256, 4) clique_warp_kernel(const BJob *__restr
     g.rows = reinterpret_cast<uint32_t *>(s_rows[wib]);
     g.hkey = s_hkey[wib];
     g.hidx = s_hidx[wib];
-    g.rlo = s_rlo[wib];
-    g.rhi = s_rhi[wib];
+    g.rext = s_rext[wib];
     g.W = W;
     g.W64 = W64;
     g.S = S;
@@ -570,12 +598,14 @@ __host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads) {
 
 // Block tier: one block per start vertex; the list holds global start-vertex indices, heaviest
 // degree bucket first, and its length is read from device memory.  The mid tier runs 256-thread
-// blocks, several per SM (registers capped for that), the large tier one 1024-thread block per SM
-// (its shared memory fills the SM).
-constexpr int kMidThreads = 256, kLargeThreads = 1024;
+// blocks, several per SM (registers capped for that); the lower large tier (out-degree up to 640)
+// two 512-thread blocks per SM, so that one block's barriers and phase tails overlap the other's
+// work; the upper large tier one 1024-thread block per SM (its shared memory fills the SM).
+constexpr int kMidThreads = 256, kLargeAThreads = 512, kLargeThreads = 1024;
 constexpr int kMidMinBlocks = 5;
+constexpr int kLargeAMax = 640;
 template <bool STATS, int KMAX, int THREADS>
-__global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : kMidMinBlocks)
+__global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREADS == kLargeAThreads ? 2 : kMidMinBlocks))
     clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ list,
                                     const unsigned int *__restrict__ list_len, int dcap, unsigned long long *queue,
                                     uint64_t *rows_out, uint64_t *phase_bytes) {
@@ -589,9 +619,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : kMidMi
     g.c = smem;
     g.hkey = smem + dp;
     g.hidx = (uint16_t *)(g.hkey + T);
-    g.rlo = g.hidx + T;
-    g.rhi = g.rlo + dp;
-    g.rows = (uint32_t *)(g.rhi + dp);
+    g.rext = (uint32_t *)(g.hidx + T);  // T is a power of two >= 32: 4-byte aligned
+    g.rows = g.rext + dp;
     g.logt = logt;
     const int warps = blockDim.x >> 5;
     const int wib = threadIdx.x >> 5;
@@ -653,9 +682,19 @@ BlockKernel block_kernel_of(bool stats, int kmax) {
     return stats ? (kmax == 5 ? clique_block_kernel<true, 5, THREADS> : clique_block_kernel<true, 4, THREADS>)
                  : (kmax == 5 ? clique_block_kernel<false, 5, THREADS> : clique_block_kernel<false, 4, THREADS>);
 }
-// tier 0: mid, tier 1: large
+// tier 0: mid, tier 1: lower large, tier 2: upper large
 BlockKernel block_kernel(bool stats, int kmax, int tier) {
-    return tier == 0 ? block_kernel_of<kMidThreads>(stats, kmax) : block_kernel_of<kLargeThreads>(stats, kmax);
+    return tier == 0   ? block_kernel_of<kMidThreads>(stats, kmax)
+           : tier == 1 ? block_kernel_of<kLargeAThreads>(stats, kmax)
+                       : block_kernel_of<kLargeThreads>(stats, kmax);
+}
+// out-degrees (lo, hi] of block tier t
+__host__ __device__ __forceinline__ int tier_lo(int t, int warp_max) {
+    return t == 0 ? warp_max : (t == 1 ? kMidMax : kLargeAMax);
+}
+__host__ __device__ __forceinline__ int tier_hi(int t) { return t == 0 ? kMidMax : (t == 1 ? kLargeAMax : kBlockMax); }
+__host__ __device__ __forceinline__ int tier_of(uint32_t d) {
+    return d <= (uint32_t)kMidMax ? 0 : (d <= (uint32_t)kLargeAMax ? 1 : 2);
 }
 
 // The hub triangle of one job (zeroed beforehand): one warp per hub row.
@@ -677,13 +716,12 @@ __global__ void hub_build_kernel(const uint64_t *__restrict__ off, const uint32_
 }
 
 // Block-tier lists in exact descending out-degree order, built without the host: a histogram
-// over degrees, one prefix pass, one write pass (a counting sort).  The mid list holds degrees
-// (warp_max, kMidMax], the large list (kMidMax, kBlockMax]; larger degrees go to the DFS engine.
-// Counter layout (unsigned int): hist[kCntDeg], cursor[kCntDeg], base[kCntDeg], then the two
-// list lengths.
+// over degrees, one prefix pass, one write pass (a counting sort).  Tier t's list holds the degrees
+// (tier_lo(t), tier_hi(t)]; larger degrees go to the DFS engine.  Counter layout (unsigned int):
+// hist[kCntDeg], cursor[kCntDeg], base[kCntDeg], then the tiers' list lengths.
 constexpr int kCntDeg = kBlockMax + 1;
-constexpr int kCntCursor = kCntDeg, kCntBase = 2 * kCntDeg, kCntMidLen = 3 * kCntDeg, kCntLargeLen = 3 * kCntDeg + 1;
-constexpr int kCntWords = 3 * kCntDeg + 2;
+constexpr int kCntCursor = kCntDeg, kCntBase = 2 * kCntDeg, kCntLen = 3 * kCntDeg;
+constexpr int kCntWords = 3 * kCntDeg + BitmapLaunch::kTiers;
 
 // pass 1: degree histogram of block-tier start vertices, and the level-1 extensions (v0, v1) of
 // every start vertex this engine serves (the reference counts one per scattered v1, engine.cc:924)
@@ -715,24 +753,20 @@ __global__ void classify_count_kernel(const BJob *__restrict__ jobs, int n_jobs,
 
 __global__ void classify_prefix_kernel(unsigned int *cnt, uint32_t warp_max) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned int acc = 0;
-    for (int d = kMidMax; d > (int)warp_max; --d) {
-        cnt[kCntBase + d] = acc;
-        acc += cnt[d];
+    for (int t = 0; t < BitmapLaunch::kTiers; ++t) {
+        unsigned int acc = 0;
+        for (int d = tier_hi(t); d > tier_lo(t, (int)warp_max); --d) {
+            cnt[kCntBase + d] = acc;
+            acc += cnt[d];
+        }
+        cnt[kCntLen + t] = acc;
     }
-    cnt[kCntMidLen] = acc;
-    acc = 0;
-    for (int d = kBlockMax; d > kMidMax; --d) {
-        cnt[kCntBase + d] = acc;
-        acc += cnt[d];
-    }
-    cnt[kCntLargeLen] = acc;
 }
 
 // pass 2: write each block-tier start vertex at its place in its list
 __global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs, uint64_t n_total,
-                                      uint32_t warp_max, unsigned int *cnt, uint32_t *mid_list,
-                                      uint32_t *large_list) {
+                                      uint32_t warp_max, unsigned int *cnt, uint32_t *list0, uint32_t *list1,
+                                      uint32_t *list2) {
     for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < n_total;
          gv += (uint64_t)gridDim.x * blockDim.x) {
         const int j = job_of(jobs, n_jobs, gv);
@@ -741,8 +775,8 @@ __global__ void classify_write_kernel(const BJob *__restrict__ jobs, int n_jobs,
         const uint32_t d = odeg(jobs[j].off, v);
         if (d <= warp_max || d > (uint32_t)kBlockMax) continue;
         const unsigned int pos = cnt[kCntBase + d] + atomicAdd(&cnt[kCntCursor + d], 1u);
-        if (d <= (uint32_t)kMidMax) mid_list[pos] = (uint32_t)gv;
-        else large_list[pos] = (uint32_t)gv;
+        const int t = tier_of(d);
+        (t == 0 ? list0 : (t == 1 ? list1 : list2))[pos] = (uint32_t)gv;
     }
 }
 
@@ -761,7 +795,7 @@ size_t bitmap_hub_bytes(uint32_t rows) { return sizeof(uint32_t) * hub_words(row
 
 size_t bitmap_arena_bytes(const std::vector<BJob> &jobs, uint64_t list_cap) {
     size_t b = Arena::round(sizeof(BJob) * std::max<size_t>(jobs.size(), 1)) +
-               2 * Arena::round(sizeof(uint32_t) * std::max<uint64_t>(list_cap, 1)) +
+               BitmapLaunch::kTiers * Arena::round(sizeof(uint32_t) * std::max<uint64_t>(list_cap, 1)) +
                Arena::round(sizeof(unsigned int) * kCntWords) + Arena::round(sizeof(unsigned long long) * 4);
     for (const auto &j : jobs) b += Arena::round(sizeof(uint32_t) * hub_words(j.hub_rows));
     return b;
@@ -781,11 +815,14 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
         return KHZ_ERR_ARG;
     }
     BJob *d_jobs = arena->take<BJob>(jobs.size());
-    L.mid_list = arena->take<uint32_t>(list_cap);
-    L.large_list = arena->take<uint32_t>(list_cap);
+    bool lists_ok = true;
+    for (int t = 0; t < BitmapLaunch::kTiers; ++t) {
+        L.lists[t] = arena->take<uint32_t>(list_cap);
+        lists_ok = lists_ok && L.lists[t];
+    }
     L.cnt = arena->take<unsigned int>(kCntWords);
     L.queues = arena->take<unsigned long long>(4);
-    if (!d_jobs || !L.mid_list || !L.large_list || !L.cnt || !L.queues) {
+    if (!d_jobs || !lists_ok || !L.cnt || !L.queues) {
         set_error("bitmap launch arena too small");
         return KHZ_ERR_OOM;
     }
@@ -807,12 +844,13 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     int dev = 0;
     KHZ_CUDA(cudaGetDevice(&dev));
     KHZ_CUDA(cudaDeviceGetAttribute(&L.sms, cudaDevAttrMultiProcessorCount, dev));
-    L.large_dcap = (int)std::min<uint32_t>((uint32_t)kBlockMax, std::max<uint32_t>(max_outdeg, kMidMax + 1));
-    L.has_mid = max_outdeg > L.warp_max;
-    L.has_large = max_outdeg > (uint32_t)kMidMax;
-    const int dcaps[2] = {kMidMax, L.large_dcap};
-    const int threads[2] = {kMidThreads, kLargeThreads};
-    for (int t = 0; t < 2; ++t) {
+    // each tier's shared memory is sized for the largest degree it serves in this launch
+    const int dcaps[BitmapLaunch::kTiers] = {
+        kMidMax, (int)std::min<uint32_t>((uint32_t)kLargeAMax, std::max<uint32_t>(max_outdeg, kMidMax + 1)),
+        (int)std::min<uint32_t>((uint32_t)kBlockMax, std::max<uint32_t>(max_outdeg, kLargeAMax + 1))};
+    const int threads[BitmapLaunch::kTiers] = {kMidThreads, kLargeAThreads, kLargeThreads};
+    for (int t = 0; t < BitmapLaunch::kTiers; ++t) {
+        L.has_tier[t] = max_outdeg > (uint32_t)tier_lo(t, (int)L.warp_max);
         const size_t smem = block_smem(dcaps[t], threads[t]);
         const BlockKernel kern = block_kernel(stats, L.kmax, t);
         // the attribute is per kernel, shared by every prepared launch: always allow the largest
@@ -855,13 +893,13 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
     }
     const int cgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 255) / 256, (uint64_t)L.sms * 8));
     classify_count_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, d_rows);
-    if (L.has_mid) {
+    if (L.has_tier[0]) {
         classify_prefix_kernel<<<1, 32, 0, s>>>(L.cnt, L.warp_max);
-        classify_write_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, L.mid_list,
-                                                    L.large_list);
+        classify_write_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.warp_max, L.cnt, L.lists[0],
+                                                    L.lists[1], L.lists[2]);
     }
     KHZ_CUDA(cudaGetLastError());
-    if (ls) ls->launches += L.has_mid ? 3 : 1;
+    if (ls) ls->launches += L.has_tier[0] ? 3 : 1;
     mark(0, true);
     {
         auto wk = L.stats ? (L.kmax == 5 ? clique_warp_kernel<true, 5> : clique_warp_kernel<true, 4>)
@@ -872,17 +910,17 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
     KHZ_CUDA(cudaGetLastError());
     mark(0, false);
     if (ls) ls->launches += 1;
-    const bool run[2] = {L.has_mid, L.has_large};
-    for (int t = 0; t < 2; ++t) {
-        if (!run[t]) continue;
-        const uint32_t *list = t == 0 ? L.mid_list : L.large_list;
-        const unsigned int *len = L.cnt + (t == 0 ? kCntMidLen : kCntLargeLen);
-        mark(1 + t, true);
+    // phases: the mid tier is phase 1, the two large tiers together phase 2
+    const int last_large = L.has_tier[2] ? 2 : 1;
+    for (int t = 0; t < BitmapLaunch::kTiers; ++t) {
+        if (!L.has_tier[t]) continue;
+        const int phase = t == 0 ? 1 : 2;
+        if (t != 2 || !L.has_tier[1]) mark(phase, true);
         const BlockKernel bk = block_kernel(L.stats, L.kmax, t);
-        bk<<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(L.d_jobs, L.n_jobs, list, len, L.block_dcap[t],
-                                                                       &L.queues[1 + t], d_rows, pb(1 + t));
+        bk<<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(
+            L.d_jobs, L.n_jobs, L.lists[t], L.cnt + kCntLen + t, L.block_dcap[t], &L.queues[1 + t], d_rows, pb(phase));
         KHZ_CUDA(cudaGetLastError());
-        mark(1 + t, false);
+        if (t == 0 || t == last_large) mark(phase, false);
         if (ls) ls->launches += 1;
     }
     return KHZ_OK;

@@ -5,8 +5,9 @@
 // compact embeddings and rebuilds each embedding through a parent chain.  Here one
 // warp owns one partial embedding at a time and walks its subtree depth-first: the
 // matched vertices live in registers, every materialised prefix ("cached object",
-// engine.h:592-613) lives in the warp's private slot of a global scratch arena (L2
-// resident for the common small sets), and every set operation is warp-cooperative
+// engine.h:592-613) lives in the warp's stack frame in shared memory (or, when it can hold
+// more than 256 members, in the warp's slot of a global arena), and every set operation is
+// warp-cooperative
 // (include/khz_setops.cuh).  Work distribution replaces WorkloadDistributer (engine.cc:1457-1496):
 // a unit is one level-1 candidate, i.e. one CSR entry (v0, adj[e]); warps grab
 // contiguous chunks of units from one atomic counter, so hub start vertices are split
@@ -25,18 +26,38 @@ namespace {
 
 constexpr int kOutStride = KHZ_MAX_COUNTS + 2;  // counts[6], num_ext, algo_bytes
 
+// The warp's materialised sets (slots 2..5: level prefixes, the cached set, the two-op temporary)
+// live in the warp's own shared-memory frame when the set can hold at most kSmemSlotWords members
+// (bounded before the operation runs: |A n B| <= min(|A|, |B|), |A \ B| <= |A|), else in its slot
+// of the global arena.  Deeper levels re-read these prefixes once per partial embedding, so the
+// common small ones are read at shared-memory latency.
+constexpr uint32_t kSmemSlotWords = 256;
+constexpr int kSmemSlots = 4;  // slots 2, 3, 4, 5
+// dynamic shared memory of a launch: one frame per warp (4 KiB)
+size_t dfs_smem_bytes(int threads) { return (size_t)(threads / 32) * kSmemSlots * kSmemSlotWords * sizeof(uint32_t); }
+
 struct WarpCtx {
     const Plan *plan;
     const uint64_t *off;
     const uint32_t *adj;
-    uint32_t *slot_base;  // this warp's kNumSlots * slot_cap words
+    uint32_t *slot_base;  // this warp's kNumSlots * slot_cap words of the global arena
+    uint32_t *smem_base;  // this warp's kSmemSlots * kSmemSlotWords words of shared memory
     uint32_t slot_cap;
+    uint32_t in_smem;     // bit s: slot s currently lives in shared memory
     uint32_t v[kMaxK];
     uint32_t slot_len[kNumSlots];
     uint64_t acc[KHZ_MAX_COUNTS];
     uint64_t ext;
     uint64_t bytes;
-    __device__ __forceinline__ uint32_t *slot(int s) { return slot_base + (size_t)s * slot_cap; }
+    __device__ __forceinline__ uint32_t *slot(int s) const {
+        return ((in_smem >> s) & 1u) ? smem_base + (size_t)(s - 2) * kSmemSlotWords : slot_base + (size_t)s * slot_cap;
+    }
+    // choose where slot s is written for a set of at most `bound` members, and return it
+    __device__ __forceinline__ uint32_t *place(int s, uint32_t bound) {
+        if (bound <= kSmemSlotWords) in_smem |= 1u << s;
+        else in_smem &= ~(1u << s);
+        return slot(s);
+    }
     __device__ __forceinline__ const uint32_t *nbr(uint32_t v) const { return adj + off[v]; }
     __device__ __forceinline__ uint32_t deg(uint32_t v) const { return (uint32_t)(off[v + 1] - off[v]); }
 };
@@ -100,6 +121,11 @@ __device__ ProbeResult apply_op(WarpCtx &c, int8_t op, const uint32_t *A, uint32
     return r;
 }
 
+// most members `A op N(x)` can have
+__device__ __forceinline__ uint32_t op_bound(const WarpCtx &c, int8_t op, uint32_t na, uint32_t x) {
+    return op == OP_AND ? min(na, c.deg(x)) : na;
+}
+
 // Materialise expression e (with 1 or 2 ops) into slot `dst`; returns its size.
 template <bool STATS>
 __device__ uint32_t materialise(WarpCtx &c, const SetExpr &e, int dst, const Filter &f, bool bounded) {
@@ -108,16 +134,18 @@ __device__ uint32_t materialise(WarpCtx &c, const SetExpr &e, int dst, const Fil
     base_of(c, e, A, na);
     const Filter none = {0, 0, 0, {0, 0, 0, 0}};
     __syncwarp();  // every lane is done reading the previous contents of the slots
+    const uint32_t b0 = op_bound(c, e.op[0], na, c.v[e.op_arg[0]]);
     if (e.op[1] == OP_NONE) {
-        ProbeResult r = apply_op<STATS>(c, e.op[0], A, na, c.v[e.op_arg[0]], c.slot(dst), bounded ? f : none,
+        ProbeResult r = apply_op<STATS>(c, e.op[0], A, na, c.v[e.op_arg[0]], c.place(dst, b0), bounded ? f : none,
                                         bounded);
         return r.full;
     }
-    ProbeResult t = apply_op<STATS>(c, e.op[0], A, na, c.v[e.op_arg[0]], c.slot(5), bounded ? f : none, bounded);
+    ProbeResult t = apply_op<STATS>(c, e.op[0], A, na, c.v[e.op_arg[0]], c.place(5, b0), bounded ? f : none, bounded);
     c.slot_len[5] = t.full;
     __syncwarp();
-    ProbeResult r = apply_op<STATS>(c, e.op[1], c.slot(5), t.full, c.v[e.op_arg[1]], c.slot(dst),
-                                    bounded ? f : none, bounded);
+    ProbeResult r = apply_op<STATS>(c, e.op[1], c.slot(5), t.full, c.v[e.op_arg[1]],
+                                    c.place(dst, op_bound(c, e.op[1], t.full, c.v[e.op_arg[1]])), bounded ? f : none,
+                                    bounded);
     return r.full;
 }
 
@@ -153,7 +181,8 @@ __device__ void count_last(WarpCtx &c) {
             const Filter none = {0, 0, 0, {0, 0, 0, 0}};
             // first op materialised (bounded by the term's lower bound when not instrumented)
             __syncwarp();
-            ProbeResult r0 = apply_op<STATS>(c, t.set.op[0], A, na, c.v[t.set.op_arg[0]], c.slot(5),
+            ProbeResult r0 = apply_op<STATS>(c, t.set.op[0], A, na, c.v[t.set.op_arg[0]],
+                                             c.place(5, op_bound(c, t.set.op[0], na, c.v[t.set.op_arg[0]])),
                                              STATS ? none : f, !STATS);
             __syncwarp();
             cnt = count_op<STATS>(c, t.set.op[1], c.slot(5), r0.full, c.v[t.set.op_arg[1]], f);
@@ -226,10 +255,13 @@ __global__ void __launch_bounds__(256) dfs_kernel(const DfsJob *__restrict__ job
         ((uint32_t *)s_plans)[i] = ((const uint32_t *)plans)[i];
     }
     __syncthreads();
+    extern __shared__ __align__(16) uint32_t dsm[];  // kSmemSlots * kSmemSlotWords words per warp
     const unsigned lane = lane_id();
     const uint32_t warp_global = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     WarpCtx c;
     c.slot_base = slots + (size_t)warp_global * kNumSlots * slot_cap;
+    c.smem_base = dsm + (size_t)(threadIdx.x >> 5) * kSmemSlots * kSmemSlotWords;
+    c.in_smem = 0;
     c.slot_cap = slot_cap;
     for (int k = 0; k < KHZ_MAX_COUNTS; ++k) c.acc[k] = 0;
     c.ext = 0;
@@ -299,7 +331,7 @@ __global__ void __launch_bounds__(256) dfs_kernel(const DfsJob *__restrict__ job
 khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_plans, uint64_t total_units,
                                uint32_t chunk, uint32_t *slots, uint32_t slot_cap, unsigned long long *queue,
                                uint64_t *d_raw, int blocks, int threads, cudaStream_t s) {
-    dfs_kernel<false><<<blocks, threads, 0, s>>>(d_jobs, n_jobs, d_plans, total_units, chunk, slots, slot_cap, queue,
+    dfs_kernel<false><<<blocks, threads, dfs_smem_bytes(threads), s>>>(d_jobs, n_jobs, d_plans, total_units, chunk, slots, slot_cap, queue,
                                                  d_raw, nullptr);
     KHZ_CUDA(cudaGetLastError());
     return KHZ_OK;
@@ -376,10 +408,10 @@ khz_status dfs_enqueue(const DfsLaunch &L, uint64_t *d_rows, cudaStream_t s, Lau
     uint64_t *pb = ls && ls->d_phase_bytes ? ls->d_phase_bytes + 3 : nullptr;
     if (ls && ls->ev_begin) cudaEventRecord(ls->ev_begin[3], s);
     if (L.stats)
-        dfs_kernel<true><<<L.blocks, L.threads, 0, s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk, slots,
+        dfs_kernel<true><<<L.blocks, L.threads, dfs_smem_bytes(L.threads), s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk, slots,
                                                         L.slot_cap, L.queue, d_rows, pb);
     else
-        dfs_kernel<false><<<L.blocks, L.threads, 0, s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk,
+        dfs_kernel<false><<<L.blocks, L.threads, dfs_smem_bytes(L.threads), s>>>(L.d_jobs, L.n_jobs, L.d_plans, L.total_units, L.chunk,
                                                          slots, L.slot_cap, L.queue, d_rows, pb);
     KHZ_CUDA(cudaGetLastError());
     if (ls && ls->ev_begin) {

@@ -1,0 +1,351 @@
+// Frequent labelled subgraph mining (3-FSM) on the device: the kautomine three_fsm app
+// (kautomine/three_fsm.cc:53-800) with its MNI support domains (SharedMemoryPatternDomain,
+// engine.h:303-403).
+//
+// The host side mirrors the app's level-by-level driver: single-vertex patterns, then edges,
+// wedges, triangles, four-chains and three-stars, each level's candidate labellings generated from
+// the frequent patterns of the levels before it (three_fsm.cc:315-590), a candidate frequent when
+// its support reaches the threshold.  A pattern's support is minimum-image based: for every
+// pattern vertex, the number of distinct graph vertices it is mapped to over all embeddings; the
+// support is the least of these (get_support, engine.h:384-401).
+//
+// Where the reference runs the engine once per candidate (run(..., restrict_starting_vertex_label,
+// labels[0])), the device enumerates every embedding of a level's template once for all of the
+// level's candidates: each warp owns one start vertex v0, lanes take the last vertex's candidates
+// in parallel, and an embedding whose label tuple is a candidate (one lookup in a dense table
+// indexed by the labels) sets its vertices' bits in that candidate's per-position domain bitmaps
+// (a word is read before the atomicOr, so repeated images cost no atomics).  A popcount kernel then
+// gives every (candidate, position) domain size.  Candidates whose bitmaps would not fit the memory
+// budget at once are processed in groups.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <set>
+#include <vector>
+
+#include "khz_internal.cuh"
+#include "khz_setops.cuh"
+
+namespace khz {
+namespace {
+
+constexpr int kFsmMaxLabels = 48;  // MAX_NUM_LABELS (graph_loader.h:28)
+
+enum Template : int { kEdge = 0, kWedge = 1, kTriangle = 2, kFourChain = 3, kThreeStar = 4 };
+constexpr int kPatSize[5] = {2, 3, 3, 4, 4};
+
+struct FsmArgs {
+    const uint64_t *off;
+    const uint32_t *adj;
+    const uint32_t *labels;
+    uint32_t n;
+    uint32_t L;             // number of labels
+    const int32_t *table;   // L^size entries: candidate index of a label tuple (group-local), or -1
+    const uint8_t *pre1;    // L^2: some candidate's first two labels
+    const uint8_t *pre2;    // L^3: some candidate's first three labels
+    uint32_t *domains;      // [candidate][position][words]
+    uint32_t words;         // ceil(n / 32)
+};
+
+__device__ __forceinline__ void mark(const FsmArgs &a, int cand, int pos, uint32_t v) {
+    uint32_t *w = a.domains + ((size_t)cand * 4 + pos) * a.words + (v >> 5);
+    const uint32_t bit = 1u << (v & 31);
+    if (!(*(volatile uint32_t *)w & bit)) atomicOr(w, bit);
+}
+
+__device__ __forceinline__ void mark_all(const FsmArgs &a, int cand, int k, const uint32_t *v) {
+    for (int p = 0; p < k; ++p) mark(a, cand, p, v[p]);
+}
+
+__device__ __forceinline__ bool contains(const uint32_t *list, uint32_t len, uint32_t x) {
+    const uint32_t p = lower_bound_u32(list, 0, len, x);
+    return p < len && __ldg(list + p) == x;
+}
+
+// One warp per start vertex v0; the embeddings enumerated are exactly those the app's apply()
+// inserts into its pattern domain with enable = true (three_fsm.cc:53-262):
+//   edge        v1 in N(v0)
+//   wedge       v1 in N(v0); v2 in N(v0), v2 != v1
+//   triangle    v1 in N(v0); v2 in N(v0) n N(v1)
+//   four-chain  v1 in N(v0); v2 in N(v0), v2 != v1; v3 in N(v1), v3 != v0, v3 != v2
+//   three-star  v1 in N(v0); v2 in N(v1), v2 != v0; v3 in N(v1), v3 != v0, v3 != v2
+template <int T>
+__global__ void __launch_bounds__(256) fsm_domain_kernel(FsmArgs a) {
+    const unsigned lane = lane_id();
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t L = a.L;
+    for (uint32_t v0 = warp; v0 < a.n; v0 += nwarps) {
+        const uint32_t l0 = __ldg(a.labels + v0);
+        const uint32_t *n0 = a.adj + a.off[v0];
+        const uint32_t d0 = (uint32_t)(a.off[v0 + 1] - a.off[v0]);
+        if constexpr (T == kEdge) {
+            for (uint32_t i = lane; i < d0; i += 32) {
+                const uint32_t v1 = __ldg(n0 + i);
+                const int c = a.table[l0 * L + __ldg(a.labels + v1)];
+                if (c >= 0) {
+                    const uint32_t v[2] = {v0, v1};
+                    mark_all(a, c, 2, v);
+                }
+            }
+        } else {
+        for (uint32_t i1 = 0; i1 < d0; ++i1) {
+            const uint32_t v1 = __ldg(n0 + i1);
+            const uint32_t l1 = __ldg(a.labels + v1);
+            if (!a.pre1[l0 * L + l1]) continue;
+            const uint32_t base01 = (l0 * L + l1) * L;
+            const uint32_t *n1 = a.adj + a.off[v1];
+            const uint32_t d1 = (uint32_t)(a.off[v1 + 1] - a.off[v1]);
+            if (T == kWedge || T == kTriangle) {
+                for (uint32_t i = lane; i < d0; i += 32) {
+                    const uint32_t v2 = __ldg(n0 + i);
+                    if (v2 == v1) continue;
+                    const int c = a.table[base01 + __ldg(a.labels + v2)];
+                    if (c < 0) continue;
+                    if (T == kTriangle && !contains(n1, d1, v2)) continue;
+                    const uint32_t v[3] = {v0, v1, v2};
+                    mark_all(a, c, 3, v);
+                }
+                continue;
+            }
+            // four-chain: v2 from N(v0); three-star: v2 from N(v1)
+            const uint32_t *n2s = T == kFourChain ? n0 : n1;
+            const uint32_t d2s = T == kFourChain ? d0 : d1;
+            for (uint32_t i2 = 0; i2 < d2s; ++i2) {
+                const uint32_t v2 = __ldg(n2s + i2);
+                if (T == kFourChain ? v2 == v1 : v2 == v0) continue;
+                const uint32_t l2 = __ldg(a.labels + v2);
+                if (!a.pre2[base01 + l2]) continue;
+                const uint32_t base012 = (base01 + l2) * L;
+                for (uint32_t i = lane; i < d1; i += 32) {
+                    const uint32_t v3 = __ldg(n1 + i);
+                    if (v3 == v0 || v3 == v2) continue;
+                    const int c = a.table[base012 + __ldg(a.labels + v3)];
+                    if (c < 0) continue;
+                    const uint32_t v[4] = {v0, v1, v2, v3};
+                    mark_all(a, c, 4, v);
+                }
+            }
+        }
+        }
+    }
+}
+
+// sizes of the domains: one block per (candidate, position)
+__global__ void fsm_popcount_kernel(const uint32_t *domains, uint32_t words, int k, uint32_t *sizes) {
+    const uint32_t *d = domains + ((size_t)(blockIdx.x / k) * 4 + blockIdx.x % k) * words;
+    uint32_t s = 0;
+    for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) s += __popc(d[w]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
+    __shared__ uint32_t part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
+        if (threadIdx.x == 0) sizes[blockIdx.x] = s;
+    }
+}
+
+using Labels = std::vector<uint32_t>;
+
+struct Candidate {
+    Labels canonical;
+    std::vector<Labels> automorphisms;  // non-canonical labellings of the same pattern
+};
+
+// ---- candidate generation, following three_fsm.cc:315-590 -------------------------------------
+struct Frequent {
+    std::vector<bool> vertex;
+    std::set<Labels> edge, wedge, triangle, chain, star;
+};
+
+std::vector<Candidate> candidates_of(int t, uint32_t L, const Frequent &f) {
+    std::vector<Candidate> out;
+    auto fe = [&](uint32_t a, uint32_t b) { return f.edge.count({a, b}) > 0; };
+    auto fw = [&](uint32_t a, uint32_t b, uint32_t c) { return f.wedge.count({a, b, c}) > 0; };
+    for (uint32_t l0 = 0; l0 < L; ++l0) {
+        if (!f.vertex[l0]) continue;
+        for (uint32_t l1 = 0; l1 < L; ++l1) {
+            if (t == kEdge) {
+                if (f.vertex[l1] && l0 <= l1) out.push_back({{l0, l1}, {{l1, l0}}});
+                continue;
+            }
+            if (!fe(l0, l1)) continue;
+            for (uint32_t l2 = 0; l2 < L; ++l2) {
+                if (t == kWedge) {
+                    if (fe(l0, l2) && l1 <= l2) out.push_back({{l0, l1, l2}, {{l0, l2, l1}}});
+                    continue;
+                }
+                if (!fw(l0, l1, l2)) continue;
+                if (t == kTriangle) {
+                    if (fw(l1, l0, l2) && fw(l2, l0, l1) && l0 <= l1 && l1 <= l2)
+                        out.push_back({{l0, l1, l2},
+                                       {{l0, l2, l1}, {l1, l0, l2}, {l1, l2, l0}, {l2, l0, l1}, {l2, l1, l0}}});
+                    continue;
+                }
+                for (uint32_t l3 = 0; l3 < L; ++l3) {
+                    if (t == kFourChain) {
+                        if (fw(l1, l0, l3) && fe(l0, l2) && fe(l1, l3) && l0 <= l1)
+                            out.push_back({{l0, l1, l2, l3}, {}});
+                    } else {  // three-star centred at l0: the canonical labelling puts the centre second
+                        if (fw(l0, l2, l3) && fw(l0, l1, l3) && l1 <= l2 && l2 <= l3)
+                            out.push_back({{l1, l0, l2, l3}, {}});
+                    }
+                }
+            }
+        }
+    }
+    return out;
+}
+
+}  // namespace
+}  // namespace khz
+
+using namespace khz;
+
+extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz_fsm_result *out,
+                              khz_fsm_pattern *patterns, uint32_t capacity, uint32_t *num_patterns) {
+    if (!out) {
+        set_error("null result");
+        return KHZ_ERR_ARG;
+    }
+    khz_graph_info gi;
+    khz_status st = khz_graph_info_get(ctx, g, &gi);
+    if (st) return st;
+    if (!gi.d_labels || gi.num_labels == 0) {
+        set_error("3-FSM needs a graph with node labels");
+        return KHZ_ERR_ARG;
+    }
+    if (gi.num_labels > (uint32_t)kFsmMaxLabels) {
+        set_error("3-FSM supports at most %d labels (the graph has %u)", kFsmMaxLabels, gi.num_labels);
+        return KHZ_ERR_ARG;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    const uint32_t n = gi.num_vertices, L = gi.num_labels;
+    memset(out, 0, sizeof(*out));
+    if (num_patterns) *num_patterns = 0;
+    auto emit = [&](int level, const Labels &lab, uint32_t support) {
+        if (!patterns || !num_patterns) return;
+        if (*num_patterns < capacity) {
+            khz_fsm_pattern &p = patterns[*num_patterns];
+            memset(&p, 0, sizeof(p));
+            p.level = level;
+            p.size = (uint32_t)lab.size();
+            for (size_t i = 0; i < lab.size(); ++i) p.labels[i] = lab[i];
+            p.support = support;
+        }
+        *num_patterns += 1;
+    };
+    // level 0: single vertices (setup, three_fsm.cc:289-310): the support sum counts every label
+    std::vector<uint32_t> h_labels(n);
+    KHZ_CUDA(cudaMemcpy(h_labels.data(), gi.d_labels, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    std::vector<uint64_t> per_label(L, 0);
+    for (uint32_t v = 0; v < n; ++v) per_label[h_labels[v]] += 1;
+    Frequent f;
+    f.vertex.assign(L, false);
+    for (uint32_t l = 0; l < L; ++l) {
+        f.vertex[l] = per_label[l] >= threshold;
+        out->level[0].num_candidates += 1;
+        out->level[0].num_frequent += f.vertex[l] ? 1 : 0;
+        out->level[0].support_sum += per_label[l];
+        if (f.vertex[l]) emit(0, {l}, (uint32_t)per_label[l]);
+    }
+    // device buffers for the label tables (sized for L^4) and the domains (grouped by budget)
+    const size_t tsize = (size_t)L * L * L * L;
+    const uint32_t words = (n + 31) / 32;
+    size_t free_b = 0, total_b = 0;
+    KHZ_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = std::max<size_t>(free_b / 4, (size_t)64 << 20);
+    const size_t per_cand = (size_t)4 * words * sizeof(uint32_t);
+    const size_t group_max = std::max<size_t>(1, budget / per_cand);
+    int32_t *d_table = nullptr;
+    uint8_t *d_pre = nullptr;
+    uint32_t *d_dom = nullptr, *d_sizes = nullptr;
+    auto release = [&]() {
+        cudaFree(d_table);
+        cudaFree(d_pre);
+        cudaFree(d_dom);
+        cudaFree(d_sizes);
+    };
+    cudaError_t e = cudaMalloc(&d_table, sizeof(int32_t) * tsize);
+    if (e == cudaSuccess) e = cudaMalloc(&d_pre, (size_t)L * L + (size_t)L * L * L);
+    if (e == cudaSuccess) e = cudaMalloc(&d_dom, per_cand * group_max);
+    if (e == cudaSuccess) e = cudaMalloc(&d_sizes, sizeof(uint32_t) * 4 * group_max);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        set_error("3-FSM device buffers: %s", cudaGetErrorString(e));
+        return KHZ_ERR_OOM;
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)n + 7) / 8, (uint64_t)sms * 16));
+    std::vector<int32_t> table(tsize);
+    std::vector<uint8_t> pre((size_t)L * L + (size_t)L * L * L);
+    for (int t = kEdge; t <= kThreeStar; ++t) {
+        const std::vector<Candidate> cands = candidates_of(t, L, f);
+        const int k = kPatSize[t];
+        khz_fsm_level &lv = out->level[1 + t];
+        lv.num_candidates = (uint32_t)cands.size();
+        std::set<Labels> *freq = t == kEdge       ? &f.edge
+                                 : t == kWedge    ? &f.wedge
+                                 : t == kTriangle ? &f.triangle
+                                 : t == kFourChain ? &f.chain
+                                                   : &f.star;
+        for (size_t g0 = 0; g0 < cands.size(); g0 += group_max) {
+            const size_t gn = std::min(group_max, cands.size() - g0);
+            std::fill(table.begin(), table.end(), -1);
+            std::fill(pre.begin(), pre.end(), 0);
+            for (size_t c = 0; c < gn; ++c) {
+                const Labels &lab = cands[g0 + c].canonical;
+                size_t idx = 0;
+                for (int p = 0; p < k; ++p) idx = idx * L + lab[p];
+                table[idx] = (int32_t)c;
+                pre[(size_t)lab[0] * L + lab[1]] = 1;
+                if (k == 4) pre[(size_t)L * L + ((size_t)lab[0] * L + lab[1]) * L + lab[2]] = 1;
+            }
+            size_t tn = 1;
+            for (int p = 0; p < k; ++p) tn *= L;
+            st = KHZ_OK;
+            if (cudaMemcpy(d_table, table.data(), sizeof(int32_t) * tn, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(d_pre, pre.data(), pre.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemset(d_dom, 0, per_cand * gn) != cudaSuccess) {
+                release();
+                return cuda_fail(cudaGetLastError(), "3-FSM tables");
+            }
+            FsmArgs a{gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_table, d_pre, d_pre + (size_t)L * L, d_dom, words};
+            switch (t) {
+                case kEdge: fsm_domain_kernel<kEdge><<<grid, 256>>>(a); break;
+                case kWedge: fsm_domain_kernel<kWedge><<<grid, 256>>>(a); break;
+                case kTriangle: fsm_domain_kernel<kTriangle><<<grid, 256>>>(a); break;
+                case kFourChain: fsm_domain_kernel<kFourChain><<<grid, 256>>>(a); break;
+                default: fsm_domain_kernel<kThreeStar><<<grid, 256>>>(a); break;
+            }
+            fsm_popcount_kernel<<<(unsigned)(gn * k), 256>>>(d_dom, words, k, d_sizes);
+            std::vector<uint32_t> sizes(gn * k);
+            e = cudaMemcpy(sizes.data(), d_sizes, sizeof(uint32_t) * gn * k, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                release();
+                return cuda_fail(e, "3-FSM domains");
+            }
+            for (size_t c = 0; c < gn; ++c) {
+                uint32_t support = n;  // get_support starts from the vertex count (engine.h:385)
+                for (int p = 0; p < k; ++p) support = std::min(support, sizes[c * k + p]);
+                if (support >= threshold) {
+                    const Candidate &cd = cands[g0 + c];
+                    freq->insert(cd.canonical);
+                    for (const Labels &aut : cd.automorphisms) freq->insert(aut);
+                    lv.num_frequent += 1;
+                    lv.support_sum += support;
+                    emit(1 + t, cd.canonical, support);
+                }
+            }
+        }
+    }
+    release();
+    out->ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return KHZ_OK;
+}

@@ -143,6 +143,28 @@ __global__ void orient_kernel(const uint64_t *__restrict__ off, const uint32_t *
     }
 }
 
+// degree-descending relabelling: new vertex q = n - 1 - r is u = order[r]; its list holds the new
+// ids of all of u's neighbours (one warp per new vertex; lists sorted afterwards)
+__global__ void relabel_degree_count_kernel(const uint64_t *__restrict__ off, const uint64_t *__restrict__ sorted_keys,
+                                            uint32_t n, uint64_t *deg) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t u = (uint32_t)sorted_keys[n - 1 - q];
+        deg[q] = off[u + 1] - off[u];
+    }
+}
+__global__ void relabel_degree_write_kernel(const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
+                                            const uint64_t *__restrict__ sorted_keys, const uint32_t *__restrict__ rank,
+                                            uint32_t n, const uint64_t *__restrict__ noff, uint32_t *nadj) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t q = warp; q < n; q += nwarps) {
+        const uint32_t u = (uint32_t)sorted_keys[n - 1 - q];
+        const uint64_t b = off[u], e = off[u + 1], o = noff[q];
+        for (uint64_t i = b + lane; i < e; i += 32) nadj[o + (i - b)] = n - 1 - rank[adj[i]];
+    }
+}
+
 __global__ void rmat_kernel(int scale, uint64_t base, uint32_t ta, uint32_t tab, uint32_t tabc, uint64_t raw,
                             uint64_t *keys) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < raw; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -369,6 +391,72 @@ khz_status orient_graph(const Graph &in, Graph *outg, cudaStream_t s) {
     out.max_degree = mx;
     out.oriented = true;
     out.symmetric = out.m == 0;
+    out.bytes = ((uint64_t)n + 1) * 8 + (out.m + kAdjPad) * 4;
+    *outg = out;
+    return KHZ_OK;
+}
+
+// The same undirected graph with vertices renumbered by descending (degree, id): new id
+// n - 1 - rank, rank being the orientation's (degree, id) order.  Every list keeps all neighbours,
+// sorted.  Counting with the smallest new id as the start vertex then starts each copy of a
+// pattern at its highest-degree vertex.
+khz_status relabel_by_degree(const Graph &in, Graph *outg, cudaStream_t s) {
+    const int sms = num_sms();
+    const uint32_t n = in.n;
+    Graph out;
+    out.n = n;
+    out.m = in.m;
+    DevBuf keys, skeys, rank, tmp;
+    KHZ_CUDA(dev_alloc(&keys.p, sizeof(uint64_t) * ((size_t)n + 1)));
+    KHZ_CUDA(dev_alloc(&skeys.p, sizeof(uint64_t) * std::max<uint32_t>(n, 1)));
+    KHZ_CUDA(dev_alloc(&rank.p, sizeof(uint32_t) * std::max<uint32_t>(n, 1)));
+    khz_status st = dalloc(&out.off, (size_t)n + 1);
+    if (st) return st;
+    st = dalloc(&out.adj, (size_t)in.m + kAdjPad);
+    if (st) {
+        free_graph_memory(&out);
+        return st;
+    }
+    KHZ_CUDA(cudaMemsetAsync(out.adj + in.m, 0xff, kAdjPad * sizeof(uint32_t), s));
+    if (n > 0) {
+        degree_keys_kernel<<<grid_for(n, sms), 256, 0, s>>>(in.off, n, (uint64_t *)keys.p);
+        size_t tb = 0, tb2 = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, tb, (uint64_t *)keys.p, (uint64_t *)skeys.p, (int)n);
+        cub::DeviceScan::ExclusiveSum(nullptr, tb2, out.off, out.off, (int)n + 1);
+        KHZ_CUDA(dev_alloc(&tmp.p, std::max(tb, tb2)));
+        KHZ_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, tb, (uint64_t *)keys.p, (uint64_t *)skeys.p, (int)n, 0, 64, s));
+        rank_kernel<<<grid_for(n, sms), 256, 0, s>>>((uint64_t *)skeys.p, n, (uint32_t *)rank.p);
+        uint64_t *deg = (uint64_t *)keys.p;
+        KHZ_CUDA(cudaMemsetAsync(deg + n, 0, sizeof(uint64_t), s));
+        relabel_degree_count_kernel<<<grid_for(n, sms), 256, 0, s>>>(in.off, (uint64_t *)skeys.p, n, deg);
+        tb2 = std::max(tb, tb2);
+        KHZ_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb2, deg, out.off, (int)n + 1, s));
+        const int wblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)n + 7) / 8, (uint64_t)sms * 16));
+        relabel_degree_write_kernel<<<wblocks, 256, 0, s>>>(in.off, in.adj, (uint64_t *)skeys.p, (uint32_t *)rank.p, n,
+                                                            out.off, out.adj);
+        KHZ_CUDA(cudaGetLastError());
+        if (in.m > 0) {
+            DevBuf sorted, stmp;
+            KHZ_CUDA(dev_alloc(&sorted.p, sizeof(uint32_t) * in.m));
+            size_t sb = 0;
+            cub::DeviceSegmentedSort::SortKeys(nullptr, sb, out.adj, (uint32_t *)sorted.p, (int64_t)in.m, (int64_t)n,
+                                               out.off, out.off + 1);
+            KHZ_CUDA(dev_alloc(&stmp.p, std::max<size_t>(sb, 1)));
+            KHZ_CUDA(cub::DeviceSegmentedSort::SortKeys(stmp.p, sb, out.adj, (uint32_t *)sorted.p, (int64_t)in.m,
+                                                        (int64_t)n, out.off, out.off + 1, s));
+            KHZ_CUDA(cudaMemcpyAsync(out.adj, sorted.p, sizeof(uint32_t) * in.m, cudaMemcpyDeviceToDevice, s));
+        }
+    } else {
+        KHZ_CUDA(cudaMemsetAsync(out.off, 0, sizeof(uint64_t), s));
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        free_graph_memory(&out);
+        return cuda_fail(e, "degree relabelling");
+    }
+    out.max_degree = in.max_degree;
+    out.symmetric = in.symmetric;
+    out.oriented = in.m == 0;
     out.bytes = ((uint64_t)n + 1) * 8 + (out.m + kAdjPad) * 4;
     *outg = out;
     return KHZ_OK;

@@ -145,6 +145,8 @@ using namespace khz;
 // involves no host synchronisation, so its launch sequence can be captured into a CUDA graph.
 struct BatchPlan {
     int rows = 0;
+    int aux_rows = 0;  // counter rows after the jobs' own, for engines feeding identity-counted jobs
+    MotifLaunch ml;
     std::vector<int> apps;
     bool stats = false;
     bool has_bitmap = false, has_dfs = false, has_wedge = false;
@@ -340,6 +342,23 @@ khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
     return KHZ_OK;
 }
 
+// degree-descending renumbering of a symmetric graph (built once, cached, freed with the graph)
+khz_status degree_view_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
+    Graph *g = get_graph(ctx, h);
+    if (!g) return KHZ_ERR_ARG;
+    if (g->degree_view == 0) {
+        Graph r;
+        AllocScope scope(ctx->pool, s);
+        khz_status st = relabel_by_degree(*g, &r, s);
+        if (st) return st;
+        khz_graph rh = add_graph(ctx, r);
+        g = get_graph(ctx, h);  // the table may have moved
+        g->degree_view = rh;
+    }
+    *out = get_graph(ctx, g->degree_view);
+    return KHZ_OK;
+}
+
 // engine for one job under the context's configuration: the bitmap engine for clique apps on
 // graphs that are a DAG in id order or symmetric (oriented once, cached); the DFS engine otherwise
 // and the wedge engine for the 4-cycle app on symmetric graphs.  Instrumented runs
@@ -349,8 +368,9 @@ khz_status oriented_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s) {
 // stored oriented, and the 3-motif identity path (global degree sums) not at all.
 int pick_engine(const khz_config &cfg, const AppDef &def, int app, const Graph &g, bool restricted = false) {
     const bool wedge_ok = app == KHZ_KGPI_4CYCLE && g.symmetric && !cfg.want_algo_bytes;
-    const bool motif3 = (app == KHZ_KAUTO_3MOTIF || app == KHZ_KGPI_3MOTIF) && g.symmetric && !cfg.want_algo_bytes &&
-                        !restricted;
+    const bool motif3 = (app == KHZ_KAUTO_3MOTIF || app == KHZ_KGPI_3MOTIF || app == KHZ_KAUTO_4MOTIF ||
+                         app == KHZ_KGPI_TAILED_TRIANGLE) &&
+                        g.symmetric && !cfg.want_algo_bytes && !restricted;
     int engine = cfg.engine;
     if (engine == KHZ_ENGINE_AUTO)
         engine = def.clique || motif3 ? KHZ_ENGINE_BITMAP : (wedge_ok ? KHZ_ENGINE_WEDGE : KHZ_ENGINE_DFS);
@@ -399,6 +419,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     P->stats = ctx->cfg.want_algo_bytes != 0;
     std::vector<BJob> bjobs;
     std::vector<MJob> mjobs;
+    std::vector<MotifJob> motif_jobs;
     std::vector<WJob> wjobs;
     std::vector<DfsJob> djobs;
     std::vector<Plan> plans;
@@ -433,7 +454,51 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         if (lab < 0)
             for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
         const int engine = pick_engine(ctx->cfg, def, jobs[i].app, g0, lab >= 0);
-        if (engine == KHZ_ENGINE_BITMAP && !def.clique) {
+        if (engine == KHZ_ENGINE_BITMAP &&
+            (jobs[i].app == KHZ_KAUTO_4MOTIF || jobs[i].app == KHZ_KGPI_TAILED_TRIANGLE)) {
+            // identities over per-edge triangle counts (motif.cu); the 4-motif's 4-cliques come from
+            // the bitmap engine and its 4-cycles from the wedge engine, each into an auxiliary row
+            Graph *og = nullptr;
+            khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
+            if (st) return st;
+            const Graph og_copy = *og;
+            MotifJob mj{};
+            mj.ooff = og_copy.off;
+            mj.oadj = og_copy.adj;
+            mj.n = og_copy.n;
+            mj.kind = jobs[i].app;
+            mj.om = og_copy.m;
+            mj.out_row = (uint32_t)i;
+            if (jobs[i].app == KHZ_KAUTO_4MOTIF) {
+                Graph *dv = nullptr;
+                st = degree_view_of(ctx, jobs[i].graph, &dv, s);
+                if (st) return st;
+                const Graph dv_copy = *dv;
+                const Graph sg = *get_graph(ctx, jobs[i].graph);
+                auto aux_row = [&]() {
+                    ext_add.push_back(0);
+                    mult.insert(mult.end(), KHZ_MAX_COUNTS, 1u);
+                    return (uint32_t)(ext_add.size() - 1);
+                };
+                mj.k4_row = aux_row();
+                mj.c4_row = aux_row();
+                bjobs.push_back(BJob{og_copy.off, og_copy.adj, og_copy.n, 4, vbase, mj.k4_row,
+                                     bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og_copy.n, og_copy.m), nullptr,
+                                     StartFilter{nullptr, 0}});
+                vbase += og_copy.n;
+                bm_entries += og_copy.m;
+                bmax = std::max(bmax, og_copy.max_degree);
+                if (og_copy.max_degree > bitmap_block_max_degree())
+                    add_dfs(og_copy, app_def(KHZ_KAUTO_4CLIQUE).plans[0], (int)mj.k4_row, bitmap_block_max_degree() + 1,
+                            StartFilter{nullptr, 0});
+                wjobs.push_back(WJob{dv_copy.off, dv_copy.adj, dv_copy.n, dv_copy.max_degree, wbase, mj.c4_row, 0,
+                                     StartFilter{nullptr, 0}, sg.off, sg.adj});
+                wbase += dv_copy.n;
+            }
+            motif_jobs.push_back(mj);
+            ext_add[i] = 0;  // the combine kernel writes the whole NumExtensions
+            P->engine = KHZ_ENGINE_BITMAP;
+        } else if (engine == KHZ_ENGINE_BITMAP && !def.clique) {
             // 3-motif: triangles on the oriented view (bitmap engine, k = 3) + degree sums
             const Graph sg = *get_graph(ctx, jobs[i].graph);
             Graph *og = nullptr;
@@ -469,8 +534,20 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             ext_add[i] = lab >= 0 ? starts : og->n;
             P->engine = KHZ_ENGINE_BITMAP;
         } else if (engine == KHZ_ENGINE_WEDGE) {
-            const Graph &g = *get_graph(ctx, jobs[i].graph);
-            wjobs.push_back(WJob{g.off, g.adj, g.n, g.max_degree, wbase, (uint32_t)i, 0, sf});
+            const Graph g = *get_graph(ctx, jobs[i].graph);
+            if (lab >= 0) {
+                // restricted: the start vertices are the stored ones, so walk the stored graph
+                wjobs.push_back(WJob{g.off, g.adj, g.n, g.max_degree, wbase, (uint32_t)i, 0, sf, nullptr, nullptr});
+            } else {
+                // every 4-cycle once, from its highest-degree vertex: wedges walked on the
+                // degree-descending renumbering (about half the schedule's on R-MAT graphs); the
+                // schedule's level-2 NumExtensions come from the stored graph by formula
+                Graph *dv = nullptr;
+                khz_status st = degree_view_of(ctx, jobs[i].graph, &dv, s);
+                if (st) return st;
+                wjobs.push_back(
+                    WJob{dv->off, dv->adj, dv->n, dv->max_degree, wbase, (uint32_t)i, 0, sf, g.off, g.adj});
+            }
             wbase += g.n;
             // depth 0 and every undirected edge once at depth 1 (restricted: depth 1 counted on the device)
             ext_add[i] = lab >= 0 ? starts : (uint64_t)g.n + g.m / 2;
@@ -488,12 +565,15 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     // every listed start vertex has more than warp_max out-edges
     const uint64_t list_cap = std::min<uint64_t>(std::max<uint64_t>(vbase, 1), bm_entries / (warp_max + 1) + 1);
     const uint64_t dfs_warps = dfs_total_warps(ctx->cfg.dfs_warps_per_sm);
-    size_t bytes = 2 * Arena::round(sizeof(uint64_t) * kRowWords * n) + Arena::round(sizeof(uint32_t) * mult.size()) +
-                   Arena::round(sizeof(uint64_t) * n) + Arena::round(sizeof(unsigned int)) +
+    const int total = (int)ext_add.size();  // job rows, then auxiliary rows of identity-counted jobs
+    P->aux_rows = total - n;
+    size_t bytes = 2 * Arena::round(sizeof(uint64_t) * kRowWords * total) + Arena::round(sizeof(uint32_t) * mult.size()) +
+                   Arena::round(sizeof(uint64_t) * total) + Arena::round(sizeof(unsigned int)) +
                    Arena::round(sizeof(uint64_t) * kPhases);
     if (P->has_bitmap) bytes += bitmap_arena_bytes(bjobs, list_cap);
     if (P->has_wedge) bytes += wedge_arena_bytes((int)wjobs.size(), wbase);
     if (!mjobs.empty()) bytes += Arena::round(sizeof(MJob) * mjobs.size());
+    if (!motif_jobs.empty()) bytes += motif_arena_bytes(motif_jobs);
     if (P->has_dfs) bytes += dfs_arena_bytes((int)djobs.size(), (int)plans.size(), dfs_warps, slot_cap, own_scratch);
     P->slot_words = P->has_dfs ? dfs_slot_words(ctx->cfg.dfs_warps_per_sm, slot_cap) : 0;
     if (over_mem_limit(ctx, bytes, "counting launch scratch")) return KHZ_ERR_OOM;
@@ -521,18 +601,20 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     }
     P->arena.base = (char *)P->mem;
     P->arena.cap = bytes;
-    P->d_raw = P->arena.take<uint64_t>((size_t)kRowWords * n);
-    P->d_final = P->arena.take<uint64_t>((size_t)kRowWords * n);
+    P->d_raw = P->arena.take<uint64_t>((size_t)kRowWords * total);
+    P->d_final = P->arena.take<uint64_t>((size_t)kRowWords * total);
     P->d_mult = P->arena.take<uint32_t>(mult.size());
-    P->d_extadd = P->arena.take<uint64_t>(n);
+    P->d_extadd = P->arena.take<uint64_t>(total);
     P->d_bad = P->arena.take<unsigned int>(1);
     P->d_phase_bytes = P->arena.take<uint64_t>(kPhases);
     KHZ_CUDA(cudaMemcpyAsync(P->d_mult, mult.data(), sizeof(uint32_t) * mult.size(), cudaMemcpyHostToDevice, s));
-    KHZ_CUDA(cudaMemcpyAsync(P->d_extadd, ext_add.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
+    KHZ_CUDA(cudaMemcpyAsync(P->d_extadd, ext_add.data(), sizeof(uint64_t) * total, cudaMemcpyHostToDevice, s));
     khz_status st = KHZ_OK;
     if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, warp_max, &P->arena, &P->bl, s);
     if (st) return st;
     if (P->has_wedge) st = wedge_prepare(wjobs, &P->arena, &P->wl, s);
+    if (st) return st;
+    if (!motif_jobs.empty()) st = motif_prepare(motif_jobs, &P->arena, &P->ml, s);
     if (st) return st;
     if (!mjobs.empty()) {
         P->d_mjobs = P->arena.take<MJob>(mjobs.size());
@@ -560,7 +642,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
 // records per-phase events; ev_begin / ev_end (may be null) bracket the counting launches.
 khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent_t ev_begin, cudaEvent_t ev_end,
                         uint32_t *shared_slots = nullptr) {
-    KHZ_CUDA(cudaMemsetAsync(P->d_raw, 0, sizeof(uint64_t) * kRowWords * P->rows, s));
+    KHZ_CUDA(cudaMemsetAsync(P->d_raw, 0, sizeof(uint64_t) * kRowWords * (P->rows + P->aux_rows), s));
     KHZ_CUDA(cudaMemsetAsync(P->d_bad, 0, sizeof(unsigned int), s));
     KHZ_CUDA(cudaMemsetAsync(P->d_phase_bytes, 0, sizeof(uint64_t) * kPhases, s));
     if (ls) ls->d_phase_bytes = P->d_phase_bytes;
@@ -577,9 +659,12 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
     }
     if (P->has_wedge) st = wedge_enqueue(P->wl, P->d_raw, s, ls);
     if (st) return st;
+    st = motif_enqueue(P->ml, P->d_raw, s, ls);  // after the 4-clique and 4-cycle counts it combines
+    if (st) return st;
     if (ev_end) KHZ_CUDA(cudaEventRecord(ev_end, s));
-    finalize_kernel<<<(unsigned)((P->rows + 127) / 128), 128, 0, s>>>(P->d_raw, P->rows, P->d_mult, P->d_extadd,
-                                                                      P->d_final, P->d_bad);
+    const int all_rows = P->rows + P->aux_rows;
+    finalize_kernel<<<(unsigned)((all_rows + 127) / 128), 128, 0, s>>>(P->d_raw, all_rows, P->d_mult, P->d_extadd,
+                                                                       P->d_final, P->d_bad);
     KHZ_CUDA(cudaGetLastError());
     if (ls) ls->launches += 1;
     return KHZ_OK;
@@ -710,7 +795,10 @@ khz_status serve_footprint(khz_server *sv, khz_graph h, int app, uint64_t *bytes
         Graph *og = nullptr;
         khz_status st = oriented_of(ctx, h, &og, nullptr);  // orient once, before any timing matters
         if (st) return st;
-        b += 2 * 4 * (og->m / 33 + 1) + bitmap_hub_bytes(bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m));
+        b += BitmapLaunch::kTiers * 4 * (og->m / 33 + 1) +
+             bitmap_hub_bytes(bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m));
+        if (app == KHZ_KAUTO_4MOTIF || app == KHZ_KGPI_TAILED_TRIANGLE)  // identity counts (motif.cu)
+            b += 4 * og->m + 16 * (uint64_t)og->n + (app == KHZ_KAUTO_4MOTIF ? 12 * (uint64_t)og->n : 0);
         if (og->max_degree > bitmap_block_max_degree())
             b += 4 * dfs_slot_words(ctx->cfg.dfs_warps_per_sm, og->max_degree);
     } else {
@@ -1254,7 +1342,7 @@ khz_status khz_graph_free(khz_ctx *ctx, khz_graph h) {
     if (!g) return KHZ_ERR_ARG;
     // work on any stream may still read the graph: order the release after all of it
     KHZ_CUDA(cudaDeviceSynchronize());
-    const khz_graph ov = g->oriented_view;
+    const khz_graph ov = g->oriented_view, dv = g->degree_view;
     // prepared launches that hold the graph's (or its oriented view's) device pointers go with it;
     // the others stay cached
     for (auto it = ctx->plans.begin(); it != ctx->plans.end();) {
@@ -1267,11 +1355,12 @@ khz_status khz_graph_free(khz_ctx *ctx, khz_graph h) {
     AllocScope scope(ctx->pool, nullptr);
     free_graph_memory(g);
     ctx->live[h - 1] = false;
-    if (ov) {
-        Graph *o = get_graph(ctx, ov);
+    for (const khz_graph view : {ov, dv}) {
+        if (!view) continue;
+        Graph *o = get_graph(ctx, view);
         if (o) {
             free_graph_memory(o);
-            ctx->live[ov - 1] = false;
+            ctx->live[view - 1] = false;
         }
     }
     return KHZ_OK;

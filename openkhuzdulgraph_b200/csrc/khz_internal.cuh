@@ -85,6 +85,7 @@ struct Graph {
     uint64_t *off = nullptr; // device n+1
     uint32_t *adj = nullptr; // device m + kAdjPad
     khz_graph oriented_view = 0;  // cached orientation of a symmetric graph (owned)
+    khz_graph degree_view = 0;    // cached degree-descending renumbering of a symmetric graph (owned)
     uint64_t bytes = 0;
     // optional node labels (the .dgraph label section, graph_loader.h:773-822): device n uint32,
     // labels dense in [0, num_labels), and the number of vertices of each label (host)
@@ -151,16 +152,17 @@ struct BitmapLaunch {
     const BJob *d_jobs = nullptr;
     int n_jobs = 0;
     uint64_t n_total = 0;
-    uint32_t *mid_list = nullptr, *large_list = nullptr;
+    // block tiers: 0 mid, 1 lower large, 2 upper large (start-vertex lists in descending degree)
+    static constexpr int kTiers = 3;
+    uint32_t *lists[kTiers] = {};
     unsigned int *cnt = nullptr;
     unsigned long long *queues = nullptr;
-    int large_dcap = 0;
     uint32_t warp_max = 64;  // out-degrees served by one warp (32 or 64)
     int kmax = 4;            // largest clique size among the jobs (4 or 5: selects the kernel build)
-    bool has_mid = false, has_large = false, stats = false;
+    bool has_tier[kTiers] = {}, stats = false;
     int sms = 0;
-    size_t block_smem[2] = {0, 0};
-    int block_threads[2] = {0, 0}, block_grid[2] = {0, 0}, block_dcap[2] = {0, 0};
+    size_t block_smem[kTiers] = {};
+    int block_threads[kTiers] = {}, block_grid[kTiers] = {}, block_dcap[kTiers] = {};
     std::vector<BJob> hubs;  // jobs with a hub triangle to build before the counting kernels
 };
 
@@ -174,6 +176,11 @@ struct WJob {
     uint32_t out_row;
     uint32_t pad2;
     StartFilter start;  // start-vertex label restriction (then the level-1 extensions are counted on the device)
+    // When off/adj are the degree-descending renumbering of the stored graph, the wedges walked are
+    // not the schedule's level-2 embeddings: these point at the stored graph, whose level-2
+    // NumExtensions are then summed by a formula (null: the walked wedges are the schedule's)
+    const uint64_t *ext_off;
+    const uint32_t *ext_adj;
 };
 
 struct WedgeLaunch {
@@ -184,6 +191,35 @@ struct WedgeLaunch {
     unsigned int *cnt = nullptr;
     unsigned long long *queues = nullptr;
     bool wide = false;           // 32-bit window counters (some degree reaches 65535)
+    bool ext_formula = false;    // some job counts on a renumbered graph (WJob::ext_off)
+    int sms = 0;
+};
+
+// One 4-vertex-pattern job counted from identities (the vertex-induced 4-motif and the tailed
+// triangle on a symmetric graph): per-edge triangle counts on the oriented view give the triangle,
+// diamond and tailed-triangle terms, degrees the star and path terms; the 4-clique and 4-cycle
+// counts come from the bitmap and wedge engines into auxiliary counter rows.
+struct MotifJob {
+    const uint64_t *ooff;  // oriented view
+    const uint32_t *oadj;
+    uint32_t n;
+    int32_t kind;          // KHZ_KAUTO_4MOTIF or KHZ_KGPI_TAILED_TRIANGLE
+    uint64_t om;           // oriented edges (= undirected edges)
+    uint32_t out_row;      // the job's counter row
+    uint32_t k4_row, c4_row;  // auxiliary rows (4-motif only)
+    uint32_t pad;
+    uint32_t *tri;         // per oriented edge: triangles on it (om)
+    unsigned long long *acc;  // per vertex: sum of its edges' triangle counts (n)
+    uint32_t *deg;         // per vertex: undirected degree (n)
+    unsigned long long *sums;  // kMotifSums accumulators
+};
+constexpr int kMotifSums = 8;
+
+struct MotifLaunch {
+    const MotifJob *d_jobs = nullptr;
+    int n_jobs = 0;
+    std::vector<MotifJob> jobs;  // host copy (grid sizes)
+    unsigned long long *queue = nullptr;  // vertex claims of the triangle kernel, one per job
     int sms = 0;
 };
 
@@ -227,6 +263,7 @@ khz_status cuda_fail(cudaError_t e, const char *what);
 khz_status build_csr_from_device_pairs(const uint32_t *d_pairs, uint64_t m, uint32_t n, bool validate,
                                        Graph *g, cudaStream_t s);
 khz_status orient_graph(const Graph &in, Graph *out, cudaStream_t s);
+khz_status relabel_by_degree(const Graph &in, Graph *out, cudaStream_t s);
 khz_status generate_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
                          Graph *g, cudaStream_t s);
 void free_graph_memory(Graph *g);
@@ -263,6 +300,9 @@ khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_p
 // DfsJob::min_deg.  No host synchronisation in bitmap_enqueue.
 // Wedge engine (4-cycle on symmetric graphs): adds each job's count (row[0]) and its level-2
 // NumExtensions (row[6]); no host synchronisation in wedge_enqueue.
+size_t motif_arena_bytes(const std::vector<MotifJob> &jobs);
+khz_status motif_prepare(std::vector<MotifJob> jobs, Arena *arena, MotifLaunch *ml, cudaStream_t s);
+khz_status motif_enqueue(const MotifLaunch &ml, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 size_t wedge_arena_bytes(int n_jobs, uint64_t n_total);
 khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunch *wl, cudaStream_t s);
 khz_status wedge_enqueue(const WedgeLaunch &wl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);

@@ -78,11 +78,47 @@ __global__ void wedge_classify_kernel(const WJob *__restrict__ jobs, int n_jobs,
         }
         for (int o = 16; o > 0; o >>= 1) wedges += __shfl_down_sync(kFull, wedges, o);
         if (lane == 0 && wedges > 0) {
-            atomicAdd((unsigned long long *)&wrow(rows, J)[KHZ_MAX_COUNTS], (unsigned long long)wedges);
+            if (!J.ext_off)  // the wedges walked are the schedule's level-2 embeddings
+                atomicAdd((unsigned long long *)&wrow(rows, J)[KHZ_MAX_COUNTS], (unsigned long long)wedges);
             const int t = wedges <= (uint64_t)kWarpWedges ? 0 : (wedges <= (uint64_t)kBlockWedges ? 1 : 2);
             const unsigned int pos = atomicAdd(&cnt[t], 1u);
             lists[(size_t)t * list_cap + pos] = (uint32_t)gv;
         }
+    }
+}
+
+// Level-2 NumExtensions of the 4-cycle schedule on the stored graph, for jobs that count on its
+// degree-descending renumbering: the level-1 embeddings (v0, v1) are the v0 < v1 in N(v1), and each
+// extends to every v2 in N(v1) above v0; with p = #{v0 in N(v1) : v0 < v1} that is
+// sum_{k < p} (deg(v1) - 1 - k) = p (deg(v1) - 1) - p (p - 1) / 2 per v1.  One thread per v1,
+// one atomic per distinct job per warp.
+__global__ void wedge_ext_formula_kernel(const WJob *__restrict__ jobs, int n_jobs, uint64_t n_total, uint64_t *rows) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;  // a multiple of 32: whole warps iterate together
+    for (uint64_t gv = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gv < ((n_total + 31) & ~31ull);
+         gv += stride) {
+        int j = -1;
+        uint64_t val = 0;
+        if (gv < n_total) {
+            j = wjob_of(jobs, n_jobs, gv);
+            const WJob &J = jobs[j];
+            if (J.ext_off) {
+                const uint32_t v = (uint32_t)(gv - J.vbase);
+                const uint64_t b = J.ext_off[v];
+                const uint64_t d = J.ext_off[v + 1] - b;
+                const uint64_t p = lower_bound_u32(J.ext_adj + b, 0, (uint32_t)d, v);
+                val = p * (d - 1) - p * (p - (p > 0 ? 1 : 0)) / 2;
+            } else {
+                j = -1;
+            }
+        }
+        const unsigned peers = __match_any_sync(kFull, j);
+        uint64_t sum = 0;
+        for (int l = 0; l < 32; ++l) {
+            const uint64_t x = __shfl_sync(kFull, val, l);
+            if ((peers >> l) & 1u) sum += x;
+        }
+        if (j >= 0 && (int)lane_id() == __ffs(peers) - 1 && sum)
+            atomicAdd((unsigned long long *)&wrow(rows, jobs[j])[KHZ_MAX_COUNTS], (unsigned long long)sum);
     }
 }
 
@@ -288,7 +324,10 @@ khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunc
         set_error("a wedge launch serves at most 2^32 - 1 start vertices");
         return KHZ_ERR_ARG;
     }
-    for (const auto &j : jobs) L.wide = L.wide || j.max_deg >= 65535u;
+    for (const auto &j : jobs) {
+        L.wide = L.wide || j.max_deg >= 65535u;
+        L.ext_formula = L.ext_formula || j.ext_off != nullptr;
+    }
     WJob *d_jobs = arena->take<WJob>(jobs.size());
     L.lists = arena->take<uint32_t>(3 * std::max<uint64_t>(L.n_total, 1));
     L.cnt = arena->take<unsigned int>(8);
@@ -320,6 +359,11 @@ khz_status wedge_enqueue(const WedgeLaunch &L, uint64_t *d_rows, cudaStream_t s,
     KHZ_CUDA(cudaMemsetAsync(L.queues, 0, sizeof(unsigned long long) * 4, s));
     const int cgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 7) / 8, (uint64_t)L.sms * 16));
     wedge_classify_kernel<<<cgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, L.cnt, L.lists, L.list_cap, d_rows);
+    if (L.ext_formula) {
+        const int fgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>((L.n_total + 255) / 256, (uint64_t)L.sms * 8));
+        wedge_ext_formula_kernel<<<fgrid, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.n_total, d_rows);
+        if (ls) ls->launches += 1;
+    }
     wedge_warp_kernel<<<L.sms * 8, 256, 0, s>>>(L.d_jobs, L.n_jobs, L.lists, L.cnt + 0, &L.queues[0], d_rows);
     wedge_block_kernel<<<L.sms * 2, kBlockThreads, 2 * kBlockSlots * sizeof(uint32_t), s>>>(
         L.d_jobs, L.n_jobs, L.lists + L.list_cap, L.cnt + 1, &L.queues[1], d_rows);

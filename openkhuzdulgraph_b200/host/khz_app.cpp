@@ -19,7 +19,38 @@ static const char *kNames[KHZ_NUM_APPS] = {
     "kgraphpi_triangle",  "kgraphpi_four_clique",  "kgraphpi_five_clique",  "kgraphpi_three_motif",
     "kgraphpi_four_cycle", "kgraphpi_house",       "kgraphpi_tailed_triangle", "kautomine_four_motif"};
 
+// kautomine_three_fsm <graph_path (*.dgraph)> <support threshold> [num_threads]: the 3-FSM app's
+// main() (kautomine/three_fsm.cc:744-800) with its per-level lines
+static int three_fsm_main(int argc, char **argv) {
+    if (argc != 4 && argc != 5) {
+        fprintf(stderr, "usage: %s kautomine_three_fsm <graph_path (*.dgraph)> <support threshold> [num_threads, default: all]\n",
+                argv[0]);
+        return 2;
+    }
+    static const char *kLevel[6] = {"single-vertex", "single-edge", "wedge", "triangle", "four-chain", "three-star"};
+    try {
+        Khuzdul::DistributedApplication application(argc == 5 ? atoi(argv[4]) : -1, argv[2], 4, KHZ_KAUTO_3MOTIF,
+                                                    true);
+        khz_fsm_result r;
+        uint32_t found = 0;
+        Khuzdul::check(khz_fsm(application.context(), application.graph(), (uint32_t)strtoul(argv[3], nullptr, 10),
+                               &r, nullptr, 0, &found));
+        printf("\nrun = 0\n");
+        for (int l = 0; l < 6; ++l)
+            printf("Number of frequent %s patterns: %u, support sum%s: %lu\n", kLevel[l], r.level[l].num_frequent,
+                   l == 0 ? "" : " of them", (unsigned long)r.level[l].support_sum);
+        printf("\n************************************************\n");
+        printf("Average runtime: %.3f (ms)\n", r.ms);
+        printf("************************************************\n\n");
+    } catch (const Khuzdul::Error &e) {
+        fprintf(stderr, "khz_app: %s\n", e.what());
+        return 1;
+    }
+    return 0;
+}
+
 int main(int argc, char **argv) {
+    if (argc >= 2 && strcmp(argv[1], "kautomine_three_fsm") == 0) return three_fsm_main(argc, argv);
     if (argc < 3 || argc > 6) {
         fprintf(stderr,
                 "usage: %s <app> <graph_path (*.dgraph)> [num_threads (-1: all threads), default: all] "

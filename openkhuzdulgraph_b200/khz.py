@@ -50,7 +50,7 @@ EXPORTS = ["khz_ctx_create", "khz_ctx_destroy", "khz_ctx_set_config", "khz_ctx_g
            "khz_batch_create", "khz_batch_launch", "khz_batch_wait", "khz_batch_destroy",
            "khz_server_create", "khz_server_submit", "khz_server_wait", "khz_server_stats_get",
            "khz_server_reset_stats", "khz_server_cancel", "khz_server_destroy", "khz_autotune",
-           "khz_app_register"]
+           "khz_app_register", "khz_fsm"]
 
 
 class KhzError(RuntimeError):
@@ -134,6 +134,22 @@ class AppDesc(ctypes.Structure):
     _fields_ = [("num_runs", ctypes.c_int32), ("num_counts", ctypes.c_int32),
                 ("multiplicity", ctypes.c_uint32 * 6), ("runs", PatternSchedule * 6)]
 
+
+class FsmLevel(ctypes.Structure):
+    _fields_ = [("num_candidates", ctypes.c_uint32), ("num_frequent", ctypes.c_uint32),
+                ("support_sum", ctypes.c_uint64)]
+
+
+class FsmResult(ctypes.Structure):
+    _fields_ = [("level", FsmLevel * 6), ("ms", ctypes.c_double)]
+
+
+class FsmPattern(ctypes.Structure):
+    _fields_ = [("level", ctypes.c_uint32), ("size", ctypes.c_uint32), ("labels", ctypes.c_uint32 * 4),
+                ("support", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+FSM_LEVELS = ["single-vertex", "single-edge", "wedge", "triangle", "four-chain", "three-star"]
 
 BASE_NBR, BASE_SET = 0, 1
 OP_NONE, OP_AND, OP_SUB = 0, 1, 2
@@ -268,6 +284,7 @@ def lib():
             "khz_server_destroy": (i32, [vp]),
             "khz_autotune": (i32, [vp, P(Job), i32, i32, P(TuneReport)]),
             "khz_app_register": (i32, [P(AppDesc), P(ctypes.c_int32)]),
+            "khz_fsm": (i32, [vp, u32, u32, P(FsmResult), P(FsmPattern), u32, P(u32)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(L, name)
@@ -413,6 +430,19 @@ class Context:
         st = Stats()
         _check(lib().khz_count_restricted(self.ptr, graph.handle, aid, label, counts, ctypes.byref(st), stream))
         return [int(counts[i]) for i in range(num_counts(aid))], st
+
+    def fsm(self, graph, threshold, capacity=4096):
+        """3-FSM (kautomine/three_fsm.cc) -> (per level {num_candidates, num_frequent, support_sum},
+        list of frequent patterns (level, labels, support), ms)"""
+        res = FsmResult()
+        pats = (FsmPattern * max(capacity, 1))()
+        num = ctypes.c_uint32(0)
+        _check(lib().khz_fsm(self.ptr, graph.handle, threshold, ctypes.byref(res), pats, capacity,
+                             ctypes.byref(num)))
+        levels = [{"num_candidates": lv.num_candidates, "num_frequent": lv.num_frequent,
+                   "support_sum": lv.support_sum} for lv in res.level]
+        found = [(p.level, list(p.labels)[:p.size], p.support) for p in pats[:min(num.value, capacity)]]
+        return levels, found, res.ms
 
     def count_async(self, graph, app, d_out_ptr, stream=None):
         _check(lib().khz_count_async(self.ptr, graph.handle, _app_id(app), d_out_ptr, stream))

@@ -1,0 +1,52 @@
+"""3-FSM on the device against the reference's own three_fsm app (tests/golden/fsm.json, written by
+tests/golden/make_fsm_golden.py from oracle/_ref/kautomine_three_fsm): per level, the number of
+frequent patterns and the support sum must be the app's."""
+import json
+import os
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+import make_fsm_golden  # noqa: E402  (the fixture's graph definitions)
+
+
+def _cases():
+    with open(os.path.join(ROOT, "tests", "golden", "fsm.json")) as f:
+        return json.load(f)["cases"]
+
+
+def test_fsm_matches_reference_app(khz_ctx):
+    graphs = {}
+    try:
+        for case in _cases():
+            spec = case["graph"]
+            if spec["name"] not in graphs:
+                sym, n, labels = make_fsm_golden.graph_of(spec)
+                g = khz_ctx.graph_from_edges(sym, n)
+                g.set_labels(labels)
+                graphs[spec["name"]] = g
+            levels, patterns, _ = khz_ctx.fsm(graphs[spec["name"]], case["threshold"])
+            for lv, (got, exp) in enumerate(zip(levels, case["levels"])):
+                assert got["num_frequent"] == exp["num_frequent"], (spec["name"], case["threshold"], lv)
+                assert got["support_sum"] == exp["support_sum"], (spec["name"], case["threshold"], lv)
+            assert len(patterns) == sum(lv["num_frequent"] for lv in levels)
+            assert all(s >= case["threshold"] for _, _, s in patterns)
+    finally:
+        for g in graphs.values():
+            g.free()
+
+
+def test_fsm_needs_labels(khz_ctx):
+    from openkhuzdulgraph_b200 import khz
+    import orc
+    canon, n = orc.er(50, 100, seed=1)
+    g = khz_ctx.graph_from_edges(orc.symmetrize(canon), n)
+    with pytest.raises(khz.KhzError) as e:
+        khz_ctx.fsm(g, 5)
+    assert e.value.status == 1
+    g.free()
