@@ -11,8 +11,11 @@ being the reference engine's own extension counter (engine.cc:924) for that sche
   flush is needed between steps.
 * e2e: the C-ABI path a user takes with host buffers: upload the oriented .dgraph edge list
   from pinned memory, device CSR build, count, copy the result back.
-* roofline: algorithmic bytes of the dominant kernel (instrumented run) / its measured time;
-  traffic = its DRAM bytes per launch from the committed ncu capture (profiles/).
+* roofline: the dominant kernel's DRAM bytes per launch (committed ncu capture, profiles/) / its
+  CUDA-event time, against the measured HBM copy bandwidth; the kernel is instruction-issue bound,
+  so the schedule's algorithmic bytes (instrumented run) / time are reported beside it, apart.
+* --workload batch | serve | configs | app | fsm: the multi-graph batch, Poisson serving, every
+  app of the full-size configurations, one app on one engine (profiling driver), and the 3-FSM.
 * cpu_baseline: the reference's own kautomine four_clique app (oracle/_ref, compiled from the
   reference's sources) on a label-restricted slice of the start vertices, all host threads.
 * --impl reference: the same reference binary as the timed arm, on the same slice.
@@ -664,14 +667,14 @@ CONFIG_RUNS = [
                                                        "kautomine_five_clique", "kgraphpi_five_clique"]),
     ("M: R-MAT s20 ef24, symmetric", 20, 24, False, ["kautomine_triangle", "kautomine_three_motif",
                                                     "kgraphpi_three_motif", "kgraphpi_four_cycle",
-                                                    "kgraphpi_tailed_triangle", "kautomine_four_motif"]),
+                                                    "kgraphpi_tailed_triangle", "kautomine_four_motif",
+                                                    "kgraphpi_house"]),
 ]
 
 
 def configs_workload(args):
     """Every app of the full-size configurations, device time per count (median of the steps), with
-    the engine each app took; the house schedule on M is left out (only the DFS engine runs it, and
-    its work grows with the square of hub degrees)."""
+    the engine each app took."""
     import torch
     from openkhuzdulgraph_b200 import khz
     torch.cuda.set_device(0)
@@ -699,6 +702,116 @@ def configs_workload(args):
             g.free()
     print(json.dumps({"metric": "device time per count, full-size configurations", "runs": out,
                       "clocks": clk.summary(), "steps": steps, "data": "synthetic (device R-MAT)"}), flush=True)
+    ctx.close()
+
+
+def app_workload(args):
+    """One app on one R-MAT graph (symmetric; degree-oriented with --oriented) with one engine:
+    device time per count (median of the steps).  The small-case driver for profiling one engine's
+    kernels, e.g. the DFS engine on the 4-motif at scale 14."""
+    import torch
+    from openkhuzdulgraph_b200 import khz
+    torch.cuda.set_device(0)
+    ctx = khz.Context(0)
+    engines = {"auto": khz.ENGINE_AUTO, "dfs": khz.ENGINE_DFS, "bitmap": khz.ENGINE_BITMAP,
+               "wedge": khz.ENGINE_WEDGE}
+    a, b, c = RMAT_ABC
+    sym = ctx.generate_rmat(args.scale, args.edge_factor, a, b, c, SEED)
+    g = sym.orient() if args.oriented else sym
+    if args.oriented:
+        sym.free()
+    ctx.set_config(engine=engines[args.engine])
+    cnt, st = ctx.count(g, args.app)
+    for _ in range(max(0, args.warmup - 1)):
+        ctx.count(g, args.app)
+    ms = []
+    with ClockSampler(0) as clk:
+        for _ in range(max(1, args.steps)):
+            c2, st = ctx.count(g, args.app)
+            assert c2 == cnt
+            ms.append(st.kernel_ms)
+    med = statistics.median(ms)
+    print(json.dumps({"metric": "device time per count", "app": args.app, "counts": cnt,
+                      "num_extensions": st.num_extensions, "ms": med, "ms_steps": ms,
+                      "engine": ["auto", "dfs", "bitmap", "wedge"][st.engine],
+                      "embeddings_per_s": (st.num_extensions + sum(cnt)) / (med / 1000), "clocks": clk.summary(),
+                      "config": {"workload": "R-MAT scale %d edge factor %d%s" % (
+                          args.scale, args.edge_factor, ", degree-oriented" if args.oriented else ""),
+                          "engine": args.engine}, "data": "synthetic (device R-MAT)"}), flush=True)
+    g.free()
+    ctx.close()
+
+
+FSM_LEVELS = ["single-vertex", "single-edge", "wedge", "triangle", "four-chain", "three-star"]
+FSM_LABELS, FSM_MULT = 5, 7919  # node label of v: (v * 7919) mod 5
+
+
+def fsm_reference(scale, edge_factor, threshold):
+    """The reference's own kautomine three_fsm (compiled unmodified into oracle/_ref) on the same
+    labelled R-MAT graph: per level (frequent patterns, support sum) and its "Average runtime"."""
+    import re
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    exe = os.path.join(orc.REF_DIR, "kautomine_three_fsm")
+    if not os.path.exists(exe):
+        return None
+    canon, n = orc.rmat(scale, edge_factor, *RMAT_ABC, seed=SEED)
+    labels = (np.arange(n, dtype=np.uint64) * FSM_MULT % FSM_LABELS).astype(np.uint32)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "fsm.dgraph")
+        orc.write_dgraph(path, n, orc.symmetrize(canon), labels)
+        out = subprocess.run([exe, path, str(threshold)], capture_output=True, text=True, timeout=3000)
+    if out.returncode != 0:
+        raise RuntimeError("reference three_fsm failed: " + out.stderr[-500:])
+    lines = re.findall(r"Number of frequent ([a-z-]+) patterns: (\d+), support sum(?: of them)?: (\d+)", out.stdout)
+    got = {k: (int(a), int(b)) for k, a, b in lines}
+    ms = float(re.search(r"Average runtime: ([0-9.]+) \(ms\)", out.stdout).group(1))
+    return {"levels": [got[k] for k in FSM_LEVELS], "ms": ms}
+
+
+def fsm_workload(args):
+    """3-FSM (kautomine/three_fsm.cc) on labelled R-MAT graphs (labels (v * 7919) mod 5, support
+    threshold 300 per 8192 vertices): host wall time of the device mining run (median of the
+    steps).  At scale 13 the reference's own three_fsm runs the same graph on the host cores: its
+    per-level frequent patterns and support sums must be the device's."""
+    import numpy as np
+    import torch
+    from openkhuzdulgraph_b200 import khz
+    torch.cuda.set_device(0)
+    ctx = khz.Context(0)
+    runs = []
+    with ClockSampler(0) as clk:
+        for scale in args.fsm_scales:
+            g = ctx.generate_rmat(scale, 16, *RMAT_ABC, SEED)
+            n = g.num_vertices
+            g.set_labels((np.arange(n, dtype=np.uint64) * FSM_MULT % FSM_LABELS).astype(np.uint32))
+            thr = max(1, 300 * n // 8192)
+            levels, pats, _ = ctx.fsm(g, thr)
+            ms = []
+            for _ in range(max(1, args.steps)):
+                lv2, _, t = ctx.fsm(g, thr)
+                assert lv2 == levels
+                ms.append(t)
+            runs.append({"graph": "R-MAT scale %d edge factor 16, %d vertices, %d labels" % (scale, n, FSM_LABELS),
+                         "threshold": thr, "ms": statistics.median(ms), "ms_steps": ms,
+                         "levels": [(lv["num_frequent"], lv["support_sum"]) for lv in levels],
+                         "candidates": [lv["num_candidates"] for lv in levels]})
+            print(json.dumps(runs[-1]), flush=True)
+            g.free()
+    ref = None
+    if not args.no_cpu and 13 in args.fsm_scales:
+        r = fsm_reference(13, 16, 300)
+        if r is not None:
+            mine = next(x for x in runs if x["threshold"] == 300)
+            assert [tuple(x) for x in mine["levels"]] == r["levels"], (mine["levels"], r["levels"])
+            model, cores, logical = host_cpu()
+            ref = {"ms": r["ms"], "levels_equal": True, "threads": max(1, logical - 2), "cores": cores,
+                   "cpu_model": model, "kind": "reference", "graph": "the scale-13 graph above",
+                   "device_over_reference": r["ms"] / mine["ms"]}
+    print(json.dumps({"metric": "3-FSM wall time per mining run", "runs": runs, "reference": ref,
+                      "clocks": clk.summary(), "steps": args.steps, "data": "synthetic (device R-MAT)"}),
+          flush=True)
     ctx.close()
 
 
@@ -750,8 +863,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="device-resident steps only (profiling)")
-    ap.add_argument("--workload", default="clique4", choices=["clique4", "batch", "serve", "configs"],
-                    help="clique4: the bench line; batch: the uneven multi-graph batch; serve: Poisson serving")
+    ap.add_argument("--workload", default="clique4",
+                    choices=["clique4", "batch", "serve", "configs", "app", "fsm"],
+                    help="clique4: the bench line; batch: the uneven multi-graph batch; serve: Poisson serving; "
+                         "configs: every app of the full-size configurations; app: one app (--app, --engine); "
+                         "fsm: 3-FSM on labelled R-MAT graphs (--fsm-scales)")
+    ap.add_argument("--fsm-scales", type=int, nargs="+", default=[13, 16, 18])
+    ap.add_argument("--app", default="kautomine_four_motif", help="app of the app workload")
+    ap.add_argument("--engine", default="auto", choices=["auto", "dfs", "bitmap", "wedge"],
+                    help="engine of the app workload")
+    ap.add_argument("--oriented", action="store_true", help="app workload: degree-oriented graph")
     ap.add_argument("--rates", type=float, nargs="+", default=[100, 500, 1000, 2000, 5000])
     ap.add_argument("--duration", type=float, default=2.0, help="seconds of arrivals per rate (serve)")
     ap.add_argument("--slots", type=int, default=4)
@@ -770,6 +891,12 @@ def main():
         return
     if args.workload == "configs":
         configs_workload(args)
+        return
+    if args.workload == "app":
+        app_workload(args)
+        return
+    if args.workload == "fsm":
+        fsm_workload(args)
         return
     if args.impl == "reference":
         # the reference arm is a CPU run on rank 0; other ranks exit without work

@@ -369,7 +369,7 @@ khz_status degree_view_of(khz_ctx *ctx, khz_graph h, Graph **out, cudaStream_t s
 int pick_engine(const khz_config &cfg, const AppDef &def, int app, const Graph &g, bool restricted = false) {
     const bool wedge_ok = app == KHZ_KGPI_4CYCLE && g.symmetric && !cfg.want_algo_bytes;
     const bool motif3 = (app == KHZ_KAUTO_3MOTIF || app == KHZ_KGPI_3MOTIF || app == KHZ_KAUTO_4MOTIF ||
-                         app == KHZ_KGPI_TAILED_TRIANGLE) &&
+                         app == KHZ_KGPI_TAILED_TRIANGLE || app == KHZ_KGPI_HOUSE) &&
                         g.symmetric && !cfg.want_algo_bytes && !restricted;
     int engine = cfg.engine;
     if (engine == KHZ_ENGINE_AUTO)
@@ -421,6 +421,7 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     std::vector<MJob> mjobs;
     std::vector<MotifJob> motif_jobs;
     std::vector<WJob> wjobs;
+    std::vector<std::pair<size_t, size_t>> house_wjobs;  // (wedge job, motif job) of each house job
     std::vector<DfsJob> djobs;
     std::vector<Plan> plans;
     std::vector<uint64_t> ext_add(n, 0);
@@ -454,10 +455,11 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
         if (lab < 0)
             for (int c = 0; c < def.num_counts; ++c) mult[(size_t)i * KHZ_MAX_COUNTS + c] = def.mult[c];
         const int engine = pick_engine(ctx->cfg, def, jobs[i].app, g0, lab >= 0);
-        if (engine == KHZ_ENGINE_BITMAP &&
-            (jobs[i].app == KHZ_KAUTO_4MOTIF || jobs[i].app == KHZ_KGPI_TAILED_TRIANGLE)) {
+        if (engine == KHZ_ENGINE_BITMAP && (jobs[i].app == KHZ_KAUTO_4MOTIF ||
+                                            jobs[i].app == KHZ_KGPI_TAILED_TRIANGLE || jobs[i].app == KHZ_KGPI_HOUSE)) {
             // identities over per-edge triangle counts (motif.cu); the 4-motif's 4-cliques come from
-            // the bitmap engine and its 4-cycles from the wedge engine, each into an auxiliary row
+            // the bitmap engine and its 4-cycles from the wedge engine, each into an auxiliary row;
+            // the house's 4-cycles and their edge-triangle sum from one weighted wedge job
             Graph *og = nullptr;
             khz_status st = oriented_of(ctx, jobs[i].graph, &og, s);
             if (st) return st;
@@ -469,17 +471,35 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
             mj.kind = jobs[i].app;
             mj.om = og_copy.m;
             mj.out_row = (uint32_t)i;
+            auto aux_row = [&]() {
+                ext_add.push_back(0);
+                mult.insert(mult.end(), KHZ_MAX_COUNTS, 1u);
+                return (uint32_t)(ext_add.size() - 1);
+            };
+            if (jobs[i].app == KHZ_KGPI_HOUSE) {
+                Graph *dv = nullptr;
+                st = degree_view_of(ctx, jobs[i].graph, &dv, s);
+                if (st) return st;
+                const Graph dv_copy = *dv;
+                const Graph sg = *get_graph(ctx, jobs[i].graph);
+                mj.c4_row = aux_row();
+                mj.house_row = aux_row();
+                mj.doff = dv_copy.off;
+                mj.dadj = dv_copy.adj;
+                mj.soff = sg.off;
+                mj.sadj = sg.adj;
+                // the entry triangle counts (WJob::tri) are placed once the motif arena is laid out
+                house_wjobs.push_back({wjobs.size(), motif_jobs.size()});
+                wjobs.push_back(WJob{dv_copy.off, dv_copy.adj, dv_copy.n, dv_copy.max_degree, wbase, mj.c4_row,
+                                     mj.house_row, StartFilter{nullptr, 0}, nullptr, nullptr, nullptr});
+                wbase += dv_copy.n;
+            }
             if (jobs[i].app == KHZ_KAUTO_4MOTIF) {
                 Graph *dv = nullptr;
                 st = degree_view_of(ctx, jobs[i].graph, &dv, s);
                 if (st) return st;
                 const Graph dv_copy = *dv;
                 const Graph sg = *get_graph(ctx, jobs[i].graph);
-                auto aux_row = [&]() {
-                    ext_add.push_back(0);
-                    mult.insert(mult.end(), KHZ_MAX_COUNTS, 1u);
-                    return (uint32_t)(ext_add.size() - 1);
-                };
                 mj.k4_row = aux_row();
                 mj.c4_row = aux_row();
                 bjobs.push_back(BJob{og_copy.off, og_copy.adj, og_copy.n, 4, vbase, mj.k4_row,
@@ -612,9 +632,10 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     khz_status st = KHZ_OK;
     if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, warp_max, &P->arena, &P->bl, s);
     if (st) return st;
-    if (P->has_wedge) st = wedge_prepare(wjobs, &P->arena, &P->wl, s);
-    if (st) return st;
     if (!motif_jobs.empty()) st = motif_prepare(motif_jobs, &P->arena, &P->ml, s);
+    if (st) return st;
+    for (const auto &hw : house_wjobs) wjobs[hw.first].tri = P->ml.jobs[hw.second].tdv;
+    if (P->has_wedge) st = wedge_prepare(wjobs, &P->arena, &P->wl, s);
     if (st) return st;
     if (!mjobs.empty()) {
         P->d_mjobs = P->arena.take<MJob>(mjobs.size());
@@ -657,9 +678,11 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
         KHZ_CUDA(cudaGetLastError());
         if (ls) ls->launches += 1;
     }
+    st = motif_enqueue_sums(P->ml, s, ls);  // before the wedge launch, which reads the house's entry counts
+    if (st) return st;
     if (P->has_wedge) st = wedge_enqueue(P->wl, P->d_raw, s, ls);
     if (st) return st;
-    st = motif_enqueue(P->ml, P->d_raw, s, ls);  // after the 4-clique and 4-cycle counts it combines
+    st = motif_enqueue_combine(P->ml, P->d_raw, s, ls);  // after the 4-clique and 4-cycle counts it combines
     if (st) return st;
     if (ev_end) KHZ_CUDA(cudaEventRecord(ev_end, s));
     const int all_rows = P->rows + P->aux_rows;
@@ -797,8 +820,9 @@ khz_status serve_footprint(khz_server *sv, khz_graph h, int app, uint64_t *bytes
         if (st) return st;
         b += BitmapLaunch::kTiers * 4 * (og->m / 33 + 1) +
              bitmap_hub_bytes(bitmap_hub_rows(ctx->cfg.bitmap_hub_rows, og->n, og->m));
-        if (app == KHZ_KAUTO_4MOTIF || app == KHZ_KGPI_TAILED_TRIANGLE)  // identity counts (motif.cu)
-            b += 4 * og->m + 16 * (uint64_t)og->n + (app == KHZ_KAUTO_4MOTIF ? 12 * (uint64_t)og->n : 0);
+        if (app == KHZ_KAUTO_4MOTIF || app == KHZ_KGPI_TAILED_TRIANGLE || app == KHZ_KGPI_HOUSE)  // identities
+            b += 4 * og->m + 16 * (uint64_t)og->n + (app != KHZ_KGPI_TAILED_TRIANGLE ? 12 * (uint64_t)og->n : 0) +
+                 (app == KHZ_KGPI_HOUSE ? 8 * og->m : 0);
         if (og->max_degree > bitmap_block_max_degree())
             b += 4 * dfs_slot_words(ctx->cfg.dfs_warps_per_sm, og->max_degree);
     } else {

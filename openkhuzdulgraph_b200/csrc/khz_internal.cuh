@@ -174,13 +174,17 @@ struct WJob {
     uint32_t max_deg;
     uint64_t vbase;
     uint32_t out_row;
-    uint32_t pad2;
+    uint32_t tri_row;   // with `tri`: the row whose count 0 receives sum over wedges of (c - 1)(t1 + t2)
     StartFilter start;  // start-vertex label restriction (then the level-1 extensions are counted on the device)
     // When off/adj are the degree-descending renumbering of the stored graph, the wedges walked are
     // not the schedule's level-2 embeddings: these point at the stored graph, whose level-2
     // NumExtensions are then summed by a formula (null: the walked wedges are the schedule's)
     const uint64_t *ext_off;
     const uint32_t *ext_adj;
+    // Per entry of adj: the triangles on that edge, or null.  With it, a second walk over each start
+    // vertex's wedges (v0, w, v2) adds (c - 1)(t(v0 w) + t(w v2)), c being the endpoint count of v2:
+    // summed, every 4-cycle once with the triangle counts of its four edges (the house identity)
+    const uint32_t *tri;
 };
 
 struct WedgeLaunch {
@@ -195,19 +199,27 @@ struct WedgeLaunch {
     int sms = 0;
 };
 
-// One 4-vertex-pattern job counted from identities (the vertex-induced 4-motif and the tailed
-// triangle on a symmetric graph): per-edge triangle counts on the oriented view give the triangle,
-// diamond and tailed-triangle terms, degrees the star and path terms; the 4-clique and 4-cycle
-// counts come from the bitmap and wedge engines into auxiliary counter rows.
+// One pattern job counted from identities (the vertex-induced 4-motif, the tailed triangle and
+// the house on a symmetric graph): per-edge triangle counts on the oriented view give the
+// triangle, diamond and tailed-triangle terms, degrees the star and path terms; the 4-clique and
+// 4-cycle counts (and the house's triangle-weighted 4-cycle sum) come from the bitmap and wedge
+// engines into auxiliary counter rows.
 struct MotifJob {
     const uint64_t *ooff;  // oriented view
     const uint32_t *oadj;
     uint32_t n;
-    int32_t kind;          // KHZ_KAUTO_4MOTIF or KHZ_KGPI_TAILED_TRIANGLE
+    int32_t kind;          // KHZ_KAUTO_4MOTIF, KHZ_KGPI_TAILED_TRIANGLE or KHZ_KGPI_HOUSE
     uint64_t om;           // oriented edges (= undirected edges)
     uint32_t out_row;      // the job's counter row
-    uint32_t k4_row, c4_row;  // auxiliary rows (4-motif only)
-    uint32_t pad;
+    uint32_t k4_row, c4_row;  // auxiliary rows: 4-cliques (4-motif), 4-cycles (4-motif, house)
+    uint32_t house_row;    // auxiliary row: the 4-cycles' edge-triangle sum (house)
+    // house only: the degree-descending renumbering walked by the wedge engine (vertex x is the
+    // oriented view's n - 1 - x), the triangle count of each of its entries, and the stored graph
+    const uint64_t *doff;
+    const uint32_t *dadj;
+    uint32_t *tdv;
+    const uint64_t *soff;
+    const uint32_t *sadj;
     uint32_t *tri;         // per oriented edge: triangles on it (om)
     unsigned long long *acc;  // per vertex: sum of its edges' triangle counts (n)
     uint32_t *deg;         // per vertex: undirected degree (n)
@@ -302,7 +314,10 @@ khz_status dfs_launch_prealloc(const DfsJob *d_jobs, int n_jobs, const Plan *d_p
 // NumExtensions (row[6]); no host synchronisation in wedge_enqueue.
 size_t motif_arena_bytes(const std::vector<MotifJob> &jobs);
 khz_status motif_prepare(std::vector<MotifJob> jobs, Arena *arena, MotifLaunch *ml, cudaStream_t s);
-khz_status motif_enqueue(const MotifLaunch &ml, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
+// the per-edge and per-vertex sums (before the wedge launch, which reads the house's entry
+// triangle counts), then the combination (after the 4-clique and 4-cycle counts it reads)
+khz_status motif_enqueue_sums(const MotifLaunch &ml, cudaStream_t s, LaunchStats *ls);
+khz_status motif_enqueue_combine(const MotifLaunch &ml, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
 size_t wedge_arena_bytes(int n_jobs, uint64_t n_total);
 khz_status wedge_prepare(const std::vector<WJob> &jobs, Arena *arena, WedgeLaunch *wl, cudaStream_t s);
 khz_status wedge_enqueue(const WedgeLaunch &wl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);

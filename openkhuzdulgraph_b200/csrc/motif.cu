@@ -1,6 +1,6 @@
-// Identity engine for the 4-vertex patterns on symmetric graphs whose schedules the DFS engine would
-// run with work growing with the square of hub degrees: the kautomine-idiom vertex-induced 4-motif
-// (six counts) and the kgraphpi tailed triangle.
+// Identity engine for the patterns on symmetric graphs whose schedules the DFS engine would run
+// with work growing with the square of hub degrees: the kautomine-idiom vertex-induced 4-motif
+// (six counts), the kgraphpi tailed triangle and the kgraphpi house.
 //
 // Non-induced counts from per-edge triangle counts t(e), per-vertex triangle counts
 // t(v) = sum_{e at v} t(e) / 2 and degrees d(v):
@@ -18,6 +18,17 @@
 //   tailed triangle (kgraphpi/four_clique.cc idiom)      n + 2 E + 3 T
 // The per-edge triangle counts come from the oriented view: each triangle a < b < c (rank order)
 // is found once, at its edge (a, b), as a common out-neighbour c, and adds one to its three edges.
+//
+// House (square v0 v1 v2 v3, roof v4 on v0 and v1; edge-induced, one automorphism broken by
+// v1 > v0): every house is one 4-cycle plus one apex over one of the cycle's edges, the apex outside
+// the cycle.  Summing over the 4-cycles the triangle counts of their four edges counts those, plus
+// the apexes inside the cycle: a cycle with a chord is a diamond, and each diamond (cycle p x q y,
+// chord x y) has one such apex on each of its four cycle edges.  So
+//   houses = sum over 4-cycles of sum over their edges of t(e)  -  4 D,
+// the first term from the wedge engine (WJob::tri), walking the degree-descending renumbering with
+// the triangle count of each of its entries.  The schedule's NumExtensions: n + E at depths 0-1,
+// sum over edges v0 < v1 of (d(v1) - 1) at depth 2, and at depth 3 each 4-cycle once per edge
+// (v3 in N(v0) n N(v2) other than v1): n + E + sum_v (d(v) - 1) #{u in N(v) : u < v} + 4 C4.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -28,7 +39,7 @@
 namespace khz {
 namespace {
 
-enum : int { kSumT3 = 0, kSumD = 1, kSumTl = 2, kSumS = 3, kSumW = 4, kSumPE = 5 };
+enum : int { kSumT3 = 0, kSumD = 1, kSumTl = 2, kSumS = 3, kSumW = 4, kSumPE = 5, kSumL2 = 6 };
 
 __device__ __forceinline__ void warp_add(unsigned long long *dst, unsigned long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
@@ -130,6 +141,48 @@ __global__ void __launch_bounds__(256) motif_path_kernel(MotifJob J) {
     warp_add(&J.sums[kSumPE], pe);
 }
 
+// House: the triangle count of every entry of the degree-descending renumbering (vertex x is the
+// oriented view's a = n - 1 - x).  x's entries below x are a's out-list in reverse order; an entry
+// y above x is the out-edge (n - 1 - y, a), found by binary search.  Warp per x.
+__global__ void __launch_bounds__(256) motif_house_entries_kernel(MotifJob J) {
+    const unsigned lane = lane_id();
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t x = warp; x < J.n; x += nw) {
+        const uint32_t a = J.n - 1 - x;
+        const uint64_t ba = J.ooff[a];
+        const uint32_t p = (uint32_t)(J.ooff[a + 1] - ba);
+        const uint64_t bx = J.doff[x];
+        const uint32_t dx = (uint32_t)(J.doff[x + 1] - bx);
+        for (uint32_t i = lane; i < dx; i += 32) {
+            uint32_t t;
+            if (i < p) {
+                t = J.tri[ba + (p - 1 - i)];
+            } else {
+                const uint32_t b = J.n - 1 - J.dadj[bx + i];
+                const uint64_t bb = J.ooff[b];
+                t = J.tri[bb + lower_bound_u32(J.oadj + bb, 0, (uint32_t)(J.ooff[b + 1] - bb), a)];
+            }
+            J.tdv[bx + i] = t;
+        }
+    }
+}
+
+// House NumExtensions at depth 2: sum over the stored graph's vertices of (d(v) - 1) times the
+// number of neighbours below v
+__global__ void motif_house_depth2_kernel(MotifJob J) {
+    unsigned long long l2 = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;  // a multiple of 32
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < ((J.n + 31) & ~31u); v += stride) {
+        if (v < J.n) {
+            const uint64_t b = J.soff[v];
+            const uint32_t d = (uint32_t)(J.soff[v + 1] - b);
+            if (d > 1) l2 += (unsigned long long)(d - 1) * lower_bound_u32(J.sadj + b, 0, d, v);
+        }
+    }
+    warp_add(&J.sums[kSumL2], l2);
+}
+
 // the job's raw counters (the finalize kernel divides by the multiplicities) and NumExtensions
 __global__ void motif_combine_kernel(MotifJob J, uint64_t *rows) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -137,6 +190,13 @@ __global__ void motif_combine_kernel(MotifJob J, uint64_t *rows) {
                     tl = (long long)J.sums[kSumTl], s = (long long)J.sums[kSumS], w = (long long)J.sums[kSumW];
     const long long n = J.n, e = (long long)J.om;
     uint64_t *row = rows + (size_t)J.out_row * kRowWords;
+    if (J.kind == KHZ_KGPI_HOUSE) {
+        const long long c4 = (long long)rows[(size_t)J.c4_row * kRowWords];
+        const long long tsum = (long long)rows[(size_t)J.house_row * kRowWords];
+        row[0] = (uint64_t)(tsum - 4 * d);
+        row[KHZ_MAX_COUNTS] = (uint64_t)(n + e + (long long)J.sums[kSumL2] + 4 * c4);
+        return;
+    }
     if (J.kind == KHZ_KGPI_TAILED_TRIANGLE) {
         row[0] = (uint64_t)tl;
         row[KHZ_MAX_COUNTS] = (uint64_t)(n + 2 * e + 3 * t);
@@ -158,11 +218,13 @@ __global__ void motif_combine_kernel(MotifJob J, uint64_t *rows) {
 size_t motif_arena_bytes(const std::vector<MotifJob> &jobs) {
     size_t b = Arena::round(sizeof(MotifJob) * std::max<size_t>(jobs.size(), 1)) +
                Arena::round(sizeof(unsigned long long) * std::max<size_t>(jobs.size(), 1));
-    for (const auto &j : jobs)
+    for (const auto &j : jobs) {
         b += Arena::round(sizeof(uint32_t) * std::max<uint64_t>(j.om, 1)) +
              Arena::round(sizeof(unsigned long long) * std::max<uint32_t>(j.n, 1)) +
              Arena::round(sizeof(uint32_t) * std::max<uint32_t>(j.n, 1)) +
              Arena::round(sizeof(unsigned long long) * kMotifSums);
+        if (j.kind == KHZ_KGPI_HOUSE) b += Arena::round(sizeof(uint32_t) * std::max<uint64_t>(2 * j.om, 1));
+    }
     return b;
 }
 
@@ -173,7 +235,8 @@ khz_status motif_prepare(std::vector<MotifJob> jobs, Arena *arena, MotifLaunch *
         j.acc = arena->take<unsigned long long>(j.n);
         j.deg = arena->take<uint32_t>(j.n);
         j.sums = arena->take<unsigned long long>(kMotifSums);
-        if (!j.tri || !j.acc || !j.deg || !j.sums) {
+        j.tdv = j.kind == KHZ_KGPI_HOUSE ? arena->take<uint32_t>(std::max<uint64_t>(2 * j.om, 1)) : nullptr;
+        if (!j.tri || !j.acc || !j.deg || !j.sums || (j.kind == KHZ_KGPI_HOUSE && !j.tdv)) {
             set_error("motif launch arena too small");
             return KHZ_ERR_OOM;
         }
@@ -193,7 +256,7 @@ khz_status motif_prepare(std::vector<MotifJob> jobs, Arena *arena, MotifLaunch *
     return KHZ_OK;
 }
 
-khz_status motif_enqueue(const MotifLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls) {
+khz_status motif_enqueue_sums(const MotifLaunch &L, cudaStream_t s, LaunchStats *ls) {
     if (L.n_jobs == 0) return KHZ_OK;
     KHZ_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(unsigned long long) * L.n_jobs, s));
     for (int i = 0; i < L.n_jobs; ++i) {
@@ -206,11 +269,24 @@ khz_status motif_enqueue(const MotifLaunch &L, uint64_t *d_rows, cudaStream_t s,
         const int vgrid = (int)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)J.n + 255) / 256, (uint64_t)L.sms * 8));
         motif_tri_kernel<<<wgrid, 256, 0, s>>>(J, L.queue + i);
         motif_edge_kernel<<<wgrid, 256, 0, s>>>(J);
-        motif_vertex_kernel<<<vgrid, 256, 0, s>>>(J);
-        if (J.kind != KHZ_KGPI_TAILED_TRIANGLE) motif_path_kernel<<<wgrid, 256, 0, s>>>(J);
-        motif_combine_kernel<<<1, 32, 0, s>>>(J, d_rows);
+        if (J.kind == KHZ_KGPI_HOUSE) {
+            motif_house_entries_kernel<<<wgrid, 256, 0, s>>>(J);
+            motif_house_depth2_kernel<<<vgrid, 256, 0, s>>>(J);
+        } else {
+            motif_vertex_kernel<<<vgrid, 256, 0, s>>>(J);
+            if (J.kind == KHZ_KAUTO_4MOTIF) motif_path_kernel<<<wgrid, 256, 0, s>>>(J);
+        }
         KHZ_CUDA(cudaGetLastError());
-        if (ls) ls->launches += J.kind != KHZ_KGPI_TAILED_TRIANGLE ? 5 : 4;
+        if (ls) ls->launches += J.kind == KHZ_KGPI_TAILED_TRIANGLE ? 3 : 4;
+    }
+    return KHZ_OK;
+}
+
+khz_status motif_enqueue_combine(const MotifLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls) {
+    for (int i = 0; i < L.n_jobs; ++i) {
+        motif_combine_kernel<<<1, 32, 0, s>>>(L.jobs[i], d_rows);
+        KHZ_CUDA(cudaGetLastError());
+        if (ls) ls->launches += 1;
     }
     return KHZ_OK;
 }

@@ -13,7 +13,13 @@
 // 512-slot shared hash (<= 384 wedges), one block with an 8192-slot shared hash (<= 6144), or one
 // 1024-thread block with dense counters in shared memory over a window of endpoint ids (106496
 // 16-bit counters, or 53248 32-bit ones when a degree reaches 65535), the endpoints v2 > v0 taken
-// one window at a time; each neighbour list's part inside the window is found by binary search.
+// one window at a time; each neighbour list's part inside the window is bounded by splitters.
+//
+// House jobs (WJob::tri set) walk each start vertex's wedges (or window) a second time once the
+// endpoint counts are final, reading them without atomics: a pair (v0, v2) with c common
+// neighbours closes C(c, 2) 4-cycles, and over those cycles each wedge (v0, w, v2) appears in c - 1,
+// so sum over wedges of (c - 1)(t(v0 w) + t(w v2)) is the sum over 4-cycles of the triangle counts
+// of their four edges.
 #include <cuda_runtime.h>
 
 #include "khz_internal.cuh"
@@ -39,6 +45,18 @@ __device__ __forceinline__ int wjob_of(const WJob *jobs, int n_jobs, uint64_t gv
 }
 
 __device__ __forceinline__ uint64_t *wrow(uint64_t *rows, const WJob &j) { return rows + (size_t)j.out_row * kRowWords; }
+
+// the count of v2 (0 if the table does not hold it; the probe visits each slot at most once)
+__device__ __forceinline__ uint32_t hash_count(const uint32_t *keys, const uint32_t *cnts, uint32_t mask,
+                                               uint32_t v2) {
+    uint32_t h = (v2 * 0x9E3779B1u) & mask;
+    for (uint32_t p = 0; p <= mask; ++p, h = (h + 1) & mask) {
+        const uint32_t k = keys[h];
+        if (k == v2) return cnts[h];
+        if (k == kEmptyKey) break;
+    }
+    return 0;
+}
 
 // add v2 to an open-addressing (key, count) table; returns the count before the increment
 __device__ __forceinline__ uint32_t hash_increment(uint32_t *keys, uint32_t *cnts, uint32_t mask, uint32_t v2) {
@@ -146,7 +164,8 @@ __device__ __forceinline__ Span splitter_span(uint32_t sp, uint32_t len, uint32_
 // the calling threads: warp `wid` of `nw` takes every nw-th w, its lanes take consecutive v2.  The
 // list bounds of a warp's next 32 w are read together (one per lane), and the next list's
 // splitters are loaded before the current list is walked, so the round trips of one w overlap the
-// previous one's work.  f(v2) is called once per wedge.
+// previous one's work.  f(v2, iw, k) is called once per wedge, iw and k being the positions in adj
+// of the entries (v0, w) and (w, v2).
 template <typename F>
 __device__ __forceinline__ void walk_wedges(const WJob &J, uint32_t v0, int wid, int nw, uint32_t lo, uint32_t hi,
                                             F f) {
@@ -171,9 +190,10 @@ __device__ __forceinline__ void walk_wedges(const WJob &J, uint32_t v0, int wid,
             if (r + 1 < nr)
                 sp_next = load_splitter(J.adj + __shfl_sync(kFull, my_b, r + 1), __shfl_sync(kFull, my_len, r + 1));
             const Span s2 = splitter_span(sp, len, lo, hi);
+            const uint64_t iw = i0 + (uint64_t)r * nw;
             for (uint64_t k = wb + s2.begin + lane; k < wb + s2.end; k += 32) {
                 const uint32_t v2 = __ldg(J.adj + k);
-                if (v2 - lo < hi - lo) f(v2);
+                if (v2 - lo < hi - lo) f(v2, iw, k);
             }
         }
     }
@@ -183,6 +203,17 @@ __device__ __forceinline__ void flush_count(uint64_t &acc, uint64_t *row) {
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
     if (lane_id() == 0 && acc) atomicAdd((unsigned long long *)&row[0], (unsigned long long)acc);
     acc = 0;
+}
+
+// the endpoint count and the weighted sum of a job, into its rows
+__device__ __forceinline__ void flush_job(uint64_t &acc, uint64_t &acc_t, uint64_t *rows, const WJob &J) {
+    flush_count(acc, wrow(rows, J));
+    if (J.tri) flush_count(acc_t, rows + (size_t)J.tri_row * kRowWords);
+}
+
+// one wedge's term of the triangle-weighted sum, c being its endpoint's count
+__device__ __forceinline__ uint64_t tri_term(const WJob &J, uint32_t c, uint64_t iw, uint64_t k) {
+    return c > 1 ? (uint64_t)(c - 1) * ((uint64_t)__ldg(J.tri + iw) + __ldg(J.tri + k)) : 0;
 }
 
 __global__ void __launch_bounds__(256) wedge_warp_kernel(const WJob *__restrict__ jobs, int n_jobs,
@@ -195,7 +226,7 @@ __global__ void __launch_bounds__(256) wedge_warp_kernel(const WJob *__restrict_
     const int wib = threadIdx.x >> 5;
     uint32_t *keys = s_keys[wib], *cnts = s_cnts[wib];
     const unsigned int n_list = *list_len;
-    uint64_t acc = 0;
+    uint64_t acc = 0, acc_t = 0;
     int cur = -1;
     while (true) {
         unsigned long long t = 0;
@@ -205,7 +236,7 @@ __global__ void __launch_bounds__(256) wedge_warp_kernel(const WJob *__restrict_
         const uint64_t gv = list[t];
         const int j = wjob_of(jobs, n_jobs, gv);
         if (j != cur) {
-            if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+            if (cur >= 0) flush_job(acc, acc_t, rows, jobs[cur]);
             cur = j;
         }
         __syncwarp();
@@ -214,11 +245,18 @@ __global__ void __launch_bounds__(256) wedge_warp_kernel(const WJob *__restrict_
             cnts[k] = 0;
         }
         __syncwarp();
-        const uint32_t v0 = (uint32_t)(gv - jobs[j].vbase);
-        walk_wedges(jobs[j], v0, 0, 1, v0 + 1, jobs[j].n,
-                    [&](uint32_t v2) { acc += hash_increment(keys, cnts, kWarpSlots - 1, v2); });
+        const WJob &J = jobs[j];
+        const uint32_t v0 = (uint32_t)(gv - J.vbase);
+        walk_wedges(J, v0, 0, 1, v0 + 1, J.n,
+                    [&](uint32_t v2, uint64_t, uint64_t) { acc += hash_increment(keys, cnts, kWarpSlots - 1, v2); });
+        if (J.tri) {
+            __syncwarp();
+            walk_wedges(J, v0, 0, 1, v0 + 1, J.n, [&](uint32_t v2, uint64_t iw, uint64_t k) {
+                acc_t += tri_term(J, hash_count(keys, cnts, kWarpSlots - 1, v2), iw, k);
+            });
+        }
     }
-    if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+    if (cur >= 0) flush_job(acc, acc_t, rows, jobs[cur]);
 }
 
 __global__ void __launch_bounds__(kBlockThreads) wedge_block_kernel(const WJob *__restrict__ jobs, int n_jobs,
@@ -230,7 +268,7 @@ __global__ void __launch_bounds__(kBlockThreads) wedge_block_kernel(const WJob *
     uint32_t *keys = smem, *cnts = smem + kBlockSlots;
     const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const unsigned int n_list = *list_len;
-    uint64_t acc = 0;
+    uint64_t acc = 0, acc_t = 0;
     int cur = -1;
     while (true) {
         if (threadIdx.x == 0) {
@@ -242,7 +280,7 @@ __global__ void __launch_bounds__(kBlockThreads) wedge_block_kernel(const WJob *
         if (gv == ~0ull) break;
         const int j = wjob_of(jobs, n_jobs, gv);
         if (j != cur) {
-            if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+            if (cur >= 0) flush_job(acc, acc_t, rows, jobs[cur]);
             cur = j;
         }
         for (int k = threadIdx.x; k < kBlockSlots; k += blockDim.x) {
@@ -250,12 +288,19 @@ __global__ void __launch_bounds__(kBlockThreads) wedge_block_kernel(const WJob *
             cnts[k] = 0;
         }
         __syncthreads();
-        const uint32_t v0 = (uint32_t)(gv - jobs[j].vbase);
-        walk_wedges(jobs[j], v0, wid, nw, v0 + 1, jobs[j].n,
-                    [&](uint32_t v2) { acc += hash_increment(keys, cnts, kBlockSlots - 1, v2); });
+        const WJob &J = jobs[j];
+        const uint32_t v0 = (uint32_t)(gv - J.vbase);
+        walk_wedges(J, v0, wid, nw, v0 + 1, J.n,
+                    [&](uint32_t v2, uint64_t, uint64_t) { acc += hash_increment(keys, cnts, kBlockSlots - 1, v2); });
         __syncthreads();
+        if (J.tri) {
+            walk_wedges(J, v0, wid, nw, v0 + 1, J.n, [&](uint32_t v2, uint64_t iw, uint64_t k) {
+                acc_t += tri_term(J, hash_count(keys, cnts, kBlockSlots - 1, v2), iw, k);
+            });
+            __syncthreads();
+        }
     }
-    if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+    if (cur >= 0) flush_job(acc, acc_t, rows, jobs[cur]);
 }
 
 // One block per heavy start vertex: the endpoints v2 in (v0, n) are counted one window of `span`
@@ -272,7 +317,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) wedge_window_kernel(const WJob
     const unsigned lane = lane_id();
     const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const unsigned int n_list = *list_len;
-    uint64_t acc = 0;
+    uint64_t acc = 0, acc_t = 0;
     int cur = -1;
     while (true) {
         if (threadIdx.x == 0) {
@@ -284,7 +329,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) wedge_window_kernel(const WJob
         if (gv == ~0ull) break;
         const int j = wjob_of(jobs, n_jobs, gv);
         if (j != cur) {
-            if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+            if (cur >= 0) flush_job(acc, acc_t, rows, jobs[cur]);
             cur = j;
         }
         const WJob &J = jobs[j];
@@ -293,7 +338,7 @@ __global__ void __launch_bounds__(kWinThreads, 1) wedge_window_kernel(const WJob
             for (uint32_t t = threadIdx.x; t < kWinWords; t += blockDim.x) win[t] = 0;
             __syncthreads();
             const uint32_t top = (uint32_t)min((uint64_t)J.n, base + span);
-            walk_wedges(J, v0, wid, nw, (uint32_t)base, top, [&](uint32_t v2) {
+            walk_wedges(J, v0, wid, nw, (uint32_t)base, top, [&](uint32_t v2, uint64_t, uint64_t) {
                 const uint32_t x = v2 - (uint32_t)base;
                 if (WIDE) {
                     acc += atomicAdd(&win[x], 1u);
@@ -303,9 +348,17 @@ __global__ void __launch_bounds__(kWinThreads, 1) wedge_window_kernel(const WJob
                 }
             });
             __syncthreads();
+            if (J.tri) {
+                walk_wedges(J, v0, wid, nw, (uint32_t)base, top, [&](uint32_t v2, uint64_t iw, uint64_t k) {
+                    const uint32_t x = v2 - (uint32_t)base;
+                    const uint32_t c = WIDE ? win[x] : (win[x >> 1] >> ((x & 1u) << 4)) & 0xffffu;
+                    acc_t += tri_term(J, c, iw, k);
+                });
+                __syncthreads();
+            }
         }
     }
-    if (cur >= 0) flush_count(acc, wrow(rows, jobs[cur]));
+    if (cur >= 0) flush_job(acc, acc_t, rows, jobs[cur]);
 }
 
 }  // namespace

@@ -420,6 +420,66 @@ def test_wedge_engine_matches_dfs_engine(khz_ctx):
         g.free()
 
 
+IDENTITY_APPS = ["kgraphpi_house", "kgraphpi_tailed_triangle", "kautomine_four_motif"]
+
+
+@pytest.mark.timeout(900, method="thread")
+def test_identity_engine_matches_dfs_engine(khz_ctx):
+    """House, tailed triangle and 4-motif on a skewed R-MAT whose hub start vertices reach every
+    wedge tier: the identity engine (per-edge triangles, weighted wedge walk) and the DFS engine
+    (the schedules as written) agree on counts and NumExtensions; on a small graph both equal the
+    oracle."""
+    from openkhuzdulgraph_b200 import khz
+    g = khz_ctx.generate_rmat(14, 16, seed=4)
+    canon, n = orc.rmat(11, 16, seed=6)
+    sym = orc.symmetrize(canon)
+    off, adj = orc.csr(sym, n)
+    g2 = khz_ctx.graph_from_edges(sym, n)
+    try:
+        for app in IDENTITY_APPS:
+            khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+            a, sa = khz_ctx.count(g, app)
+            assert sa.engine == khz.ENGINE_BITMAP, app  # the identity engine reports as the bitmap engine
+            small, ss = khz_ctx.count(g2, app)
+            khz_ctx.set_config(engine=khz.ENGINE_DFS)
+            d, sd = khz_ctx.count(g, app)
+            assert a == d and sa.num_extensions == sd.num_extensions, app
+            exp, ext, _ = orc.count(app, off, adj)
+            assert small == exp and ss.num_extensions == ext, app
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+        g.free()
+        g2.free()
+
+
+def test_house_identity_wide_window(khz_ctx):
+    """Two adjacent hubs joined to 70 000 common leaves: degrees above 65 535 put the heaviest start
+    vertex on the 32-bit window counters.  Every 4-cycle is hub-leaf-hub-leaf and every triangle's
+    apex over a cycle edge is the other hub, inside the cycle, so there are no houses while the
+    4-cycle and diamond terms are C(L, 2) each; NumExtensions follow from the degrees."""
+    from math import comb
+    ctx = khz_ctx
+    L = 70000
+    leaves = np.arange(2, L + 2, dtype=np.uint32)
+    canon = np.concatenate([np.array([[0, 1]], np.uint32), np.stack([np.zeros(L, np.uint32), leaves], 1),
+                            np.stack([np.ones(L, np.uint32), leaves], 1)])
+    n = L + 2
+    sym = orc.symmetrize(canon)
+    off, adj = orc.csr(sym, n)
+    g = ctx.graph_from_edges(sym, n)
+    try:
+        h, sh = ctx.count(g, "kgraphpi_house")
+        c4, _ = ctx.count(g, "kgraphpi_four_cycle")
+        assert c4 == [comb(L, 2)]
+        d = np.diff(off).astype(np.int64)
+        below = np.array([np.searchsorted(adj[off[v]:off[v + 1]], v) for v in range(n)], dtype=np.int64)
+        depth2 = int(((d - 1) * below).sum())
+        assert h == [0]
+        assert sh.num_extensions == n + (2 * L + 1) + depth2 + 4 * comb(L, 2)
+    finally:
+        g.free()
+
+
 def test_autotuner_keeps_counts_and_installs_settings(graphs, khz_ctx):
     from openkhuzdulgraph_b200 import khz
     jobs = [(g, app) for spec, n, sym, off, adj, g in graphs[:4]

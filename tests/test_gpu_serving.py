@@ -71,12 +71,18 @@ def test_ticket_errors(khz_ctx, resident):
 # ---- failures made on the host (no device fault is ever provoked) -------------------------------
 @pytest.fixture(scope="module")
 def heavy(khz_ctx):
-    """A graph whose house count on the DFS engine takes milliseconds, so queued queries wait."""
+    """A graph whose house count on the DFS engine takes milliseconds, so queued queries wait (the
+    context runs the schedule on the DFS engine while the fixture is alive)."""
+    from openkhuzdulgraph_b200 import khz
     canon, n = orc.rmat(13, 16, seed=9)
     g = khz_ctx.graph_from_edges(orc.symmetrize(canon), n)
-    alone = khz_ctx.count(g, "kgraphpi_house")
-    yield g, alone
-    g.free()
+    khz_ctx.set_config(engine=khz.ENGINE_DFS)
+    try:
+        alone = khz_ctx.count(g, "kgraphpi_house")
+        yield g, alone
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO)
+        g.free()
 
 
 def test_allocation_failure_reaches_tickets_without_stalling(khz_ctx, resident):
