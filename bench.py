@@ -595,21 +595,33 @@ def serve_workload(args):
     # warm: every feasible query once through the server
     for gi, app in feasible:
         sv.wait(sv.submit(graphs[gi], app), app)
+    # saturation: the same query list submitted at once vs plain sequential counting
+    qs = [rng.choice(feasible) for _ in range(args.sat_queries)]
+    sv.reset_stats()
+    t1 = time.perf_counter()
+    tk = [sv.submit(graphs[gi], app) for gi, app in qs]
+    for (gi, app), t in zip(qs, tk):
+        sv.wait(t, app, timeout_ms=600000.0)
+    served_s = time.perf_counter() - t1
+    capacity = len(qs) / served_s
+    # Poisson arrivals at the given rates, or at fractions of the measured capacity; at most
+    # --rate-queries queries per rate, so heavy mixes stay bounded in time
+    rates = args.rates if args.rates else [round(f * capacity, 1) for f in (0.25, 0.5, 0.75, 0.9)]
     rates_out = []
-    for rate in args.rates:
+    for rate in rates:
         sv.reset_stats()
-        n_q = max(50, int(rate * args.duration))
-        qs = [rng.choice(feasible) for _ in range(n_q)]
+        n_q = max(50, min(args.rate_queries, int(rate * args.duration)))
+        qs_r = [rng.choice(feasible) for _ in range(n_q)]
         arrivals = []
         t = 0.0
-        for _ in qs:
+        for _ in qs_r:
             t += rng.expovariate(rate)
             arrivals.append(t)
         tickets = [None] * n_q
 
         def submitter():
             start = time.perf_counter()
-            for k, ((gi, app), ta) in enumerate(zip(qs, arrivals)):
+            for k, ((gi, app), ta) in enumerate(zip(qs_r, arrivals)):
                 d = ta - (time.perf_counter() - start)
                 if d > 0:
                     time.sleep(d)
@@ -622,7 +634,7 @@ def serve_workload(args):
         for k in range(n_q):
             while tickets[k] is None:
                 time.sleep(0.0002)
-            gi, app = qs[k]
+            gi, app = qs_r[k]
             cnt, ext, l = sv.wait(tickets[k], app, timeout_ms=600000.0)
             assert cnt == alone[(gi, app)][0] and ext == alone[(gi, app)][1]
             lat.append(l)
@@ -632,14 +644,6 @@ def serve_workload(args):
         rates_out.append({"offered_qps": rate, "queries": n_q, "achieved_qps": n_q / wall,
                           "p50_ms": lat[len(lat) // 2], "p99_ms": lat[int(0.99 * (len(lat) - 1))],
                           "batches": sv.stats()["batches"]})
-    # saturation: the same 2000-query list submitted at once vs plain sequential counting
-    qs = [rng.choice(feasible) for _ in range(args.sat_queries)]
-    sv.reset_stats()
-    t1 = time.perf_counter()
-    tk = [sv.submit(graphs[gi], app) for gi, app in qs]
-    for (gi, app), t in zip(qs, tk):
-        sv.wait(t, app, timeout_ms=600000.0)
-    served_s = time.perf_counter() - t1
     sv.close()
     t1 = time.perf_counter()
     for gi, app in qs:
@@ -720,7 +724,8 @@ def app_workload(args):
     g = sym.orient() if args.oriented else sym
     if args.oriented:
         sym.free()
-    ctx.set_config(engine=engines[args.engine])
+    settings = {k: int(v) for k, v in (kv.split("=", 1) for kv in args.set)}
+    ctx.set_config(engine=engines[args.engine], **settings)
     cnt, st = ctx.count(g, args.app)
     for _ in range(max(0, args.warmup - 1)):
         ctx.count(g, args.app)
@@ -737,7 +742,8 @@ def app_workload(args):
                       "embeddings_per_s": (st.num_extensions + sum(cnt)) / (med / 1000), "clocks": clk.summary(),
                       "config": {"workload": "R-MAT scale %d edge factor %d%s" % (
                           args.scale, args.edge_factor, ", degree-oriented" if args.oriented else ""),
-                          "engine": args.engine}, "data": "synthetic (device R-MAT)"}), flush=True)
+                          "engine": args.engine, "settings": settings}, "data": "synthetic (device R-MAT)"}),
+          flush=True)
     g.free()
     ctx.close()
 
@@ -794,6 +800,7 @@ def fsm_workload(args):
                 assert lv2 == levels
                 ms.append(t)
             runs.append({"graph": "R-MAT scale %d edge factor 16, %d vertices, %d labels" % (scale, n, FSM_LABELS),
+                         "scale": scale,
                          "threshold": thr, "ms": statistics.median(ms), "ms_steps": ms,
                          "levels": [(lv["num_frequent"], lv["support_sum"]) for lv in levels],
                          "candidates": [lv["num_candidates"] for lv in levels]})
@@ -801,9 +808,9 @@ def fsm_workload(args):
             g.free()
     ref = None
     if not args.no_cpu and 13 in args.fsm_scales:
-        r = fsm_reference(13, 16, 300)
+        mine = runs[args.fsm_scales.index(13)]
+        r = fsm_reference(13, 16, mine["threshold"])
         if r is not None:
-            mine = next(x for x in runs if x["threshold"] == 300)
             assert [tuple(x) for x in mine["levels"]] == r["levels"], (mine["levels"], r["levels"])
             model, cores, logical = host_cpu()
             ref = {"ms": r["ms"], "levels_equal": True, "threads": max(1, logical - 2), "cores": cores,
@@ -868,17 +875,22 @@ def main():
                     help="clique4: the bench line; batch: the uneven multi-graph batch; serve: Poisson serving; "
                          "configs: every app of the full-size configurations; app: one app (--app, --engine); "
                          "fsm: 3-FSM on labelled R-MAT graphs (--fsm-scales)")
-    ap.add_argument("--fsm-scales", type=int, nargs="+", default=[13, 16, 18])
+    ap.add_argument("--fsm-scales", type=int, nargs="+", default=[13, 14])
     ap.add_argument("--app", default="kautomine_four_motif", help="app of the app workload")
     ap.add_argument("--engine", default="auto", choices=["auto", "dfs", "bitmap", "wedge"],
                     help="engine of the app workload")
     ap.add_argument("--oriented", action="store_true", help="app workload: degree-oriented graph")
-    ap.add_argument("--rates", type=float, nargs="+", default=[100, 500, 1000, 2000, 5000])
+    ap.add_argument("--set", nargs="*", default=[], metavar="KEY=VALUE",
+                    help="app workload: khz_config fields, e.g. dfs_warps_per_sm=24")
+    ap.add_argument("--rates", type=float, nargs="*", default=[],
+                    help="serve: offered rates in queries/s (default: 0.25, 0.5, 0.75 and 0.9 of the measured capacity)")
+    ap.add_argument("--rate-queries", type=int, default=400, help="serve: at most this many queries per rate")
     ap.add_argument("--duration", type=float, default=2.0, help="seconds of arrivals per rate (serve)")
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--max-batch", type=int, default=64)
-    ap.add_argument("--query-cap-ms", type=float, default=100.0)
-    ap.add_argument("--sat-queries", type=int, default=2000)
+    ap.add_argument("--query-cap-ms", type=float, default=1000.0,
+                    help="serve: a (graph, app) pair is served when that query alone takes at most this long")
+    ap.add_argument("--sat-queries", type=int, default=500)
     ap.add_argument("--graphs", type=int, default=20000, help="graphs in the batch workload")
     ap.add_argument("--scale", type=int, default=SCALE, help="R-MAT scale (the bench workload is 22)")
     ap.add_argument("--edge-factor", type=int, default=EDGE_FACTOR, help="R-MAT edge factor (workload: 16)")

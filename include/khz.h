@@ -114,7 +114,10 @@ typedef struct khz_config {
     int32_t device_mem_limit_mib; /* cap on the device memory the context holds for graphs and counting
                                      scratch, in MiB (0 = none): an allocation that would exceed it
                                      fails with KHZ_ERR_OOM, as if the device were that small */
-    int32_t reserved[8];
+    int32_t bitmap_tensor_cores;  /* bitmap engine, out-degrees above 256: 1 = count 4-cliques as a
+                                     masked 0/1 matrix product on the tensor cores; 0 (auto) or -1 =
+                                     per-edge popcounts on the CUDA cores */
+    int32_t reserved[7];
 } khz_config;
 
 /* ---- context ---------------------------------------------------------------------- */

@@ -464,6 +464,155 @@ __device__ void count_rows_small(const Local &g, int K, const uint64_t *off, Acc
     deal_flush<STATS, KMAX>(g, K, off, pc, my_i, my_j, a);
 }
 
+// ---- Tensor-core 4-clique count (large block tiers) -------------------------------------------
+// The induced subgraphs of the large tiers are dense (31 % of candidate pairs are edges for
+// 256 < d <= 640 and 44 % above that on R-MAT s22), so their 4-cliques are counted as a masked
+// matrix product: with A the d x d upper-triangular 0/1 matrix of the rows,
+//   4-cliques through v0 = sum over i < j with A[i][j] = 1 of (A A^T)[i][j]
+// (row i and row j share (A A^T)[i][j] columns, each closing a 4-clique).  A A^T runs on the
+// tensor cores as tcgen05.mma kind::i8 (0/1 bytes, int32 accumulators in tensor memory) over
+// 128 x 128 tiles of row blocks (ib, jb >= ib), only over columns >= 128 jb (row j has no bit at
+// or below j).  Per 32-column step the block expands 32 bits of each needed row into bytes in a
+// shared-memory stage (the canonical K-major layout without swizzle: 8-row core matrices of
+// 16 bytes per row, the two 16-byte K halves 2048 bytes apart), one thread issues the MMAs of up
+// to G accumulator tiles and commits them to an mbarrier, and the block waits (bounded) before the
+// stage is rewritten.  The epilogue reads each accumulator row with tcgen05.ld and adds the
+// entries whose bit is set in row i.
+constexpr int kMmaRows = 128;                 // M = N = 128 rows of the 0/1 matrix per tile
+constexpr uint32_t kMmaTileBytes = 128 * 32;  // one operand tile: 128 rows x 32 columns (bytes)
+constexpr uint32_t kMmaWaitIters = 1u << 20;  // mbarrier polls before the launch reports a stall
+constexpr int kMmaMaxTiles = 4;               // accumulator tiles per pass: 4 x 128 = all 512 TMEM columns
+// tensor-memory columns a block allocates for g accumulator tiles (a power of two >= 32)
+__host__ __device__ __forceinline__ uint32_t mma_tmem_cols(int g) { return g <= 1 ? 128u : (g == 2 ? 256u : 512u); }
+// instruction descriptor: D int32 (bits 4-5 = 2), A and B unsigned 8-bit, K-major, N = 128, M = 128
+constexpr uint32_t kMmaIdesc = (2u << 4) | ((uint32_t)(kMmaRows >> 3) << 17) | ((uint32_t)(kMmaRows >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor of one operand tile: start address, K-half stride (LBO)
+// 2048 bytes, 8-row-group stride (SBO) 128 bytes, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t mma_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(2048u >> 4) << 16) | ((uint64_t)(128u >> 4) << 32) |
+           (1ull << 46);
+}
+
+// bytes 0..3 of the result are bits 0..3 of x (as 0 / 1)
+__device__ __forceinline__ uint32_t spread4(uint32_t x) { return ((x & 0xFu) * 0x00204081u) & 0x01010101u; }
+
+// row r's 32 bits of one 32-column step as 32 bytes of the tile: bits 0-15 in the first K half,
+// bits 16-31 in the second
+__device__ __forceinline__ void expand_row_bits(uint8_t *tile, int r, uint32_t bits) {
+    const uint4 lo = make_uint4(spread4(bits), spread4(bits >> 4), spread4(bits >> 8), spread4(bits >> 12));
+    const uint4 hi = make_uint4(spread4(bits >> 16), spread4(bits >> 20), spread4(bits >> 24), spread4(bits >> 28));
+    *reinterpret_cast<uint4 *>(tile + r * 16) = lo;
+    *reinterpret_cast<uint4 *>(tile + 2048 + r * 16) = hi;
+}
+
+// true once the mbarrier's phase `parity` has completed, false after kMmaWaitIters polls
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kMmaWaitIters && !done; ++it)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+    return done != 0;
+}
+
+struct MmaState {
+    uint32_t tmem;    // tensor-memory base of the accumulators (G x 128 columns)
+    uint32_t mbar;    // shared address of the MMA-completion mbarrier
+    uint32_t phase;   // parity of the next completion
+    int G;            // accumulator tiles per pass
+    uint8_t *stage;   // (G + 1) operand tiles
+};
+
+// 4-clique count of one start vertex on the tensor cores.  Returns false (after recording the
+// stall in *err) if an MMA completion was not seen within the poll limit; the caller then stops.
+template <int THREADS>
+__device__ bool count_rows_mma(const Local &g, MmaState &ms, unsigned int *err, Acc &a) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = THREADS / 32;
+    const int d = g.d;
+    // triangles through v0 (NumExtensions): every set bit of every row
+    for (int i = tid; i < d; i += THREADS) {
+        const uint32_t *r = g.rows + (size_t)i * g.S;
+        uint32_t c = 0;
+        for (int w = (i + 1) >> 5; w < g.W; ++w) c += __popc(r[w]);
+        a.t3 += c;
+    }
+    const int nb = (d + kMmaRows - 1) / kMmaRows;
+    const int kw = g.W;  // 32-column steps
+    for (int ib = 0; ib < nb; ++ib) {
+        for (int jb0 = ib; jb0 < nb; jb0 += ms.G) {
+            const int ng = min(ms.G, nb - jb0);
+            const int k0 = jb0 * (kMmaRows / 32);
+            for (int kc = k0; kc < kw; ++kc) {
+                // stage: tile 0 = rows of block ib, tile 1 + t = rows of block jb0 + t
+                for (int task = tid; task < (ng + 1) * kMmaRows; task += THREADS) {
+                    const int tile = task / kMmaRows, r = task % kMmaRows;
+                    const int R = (tile == 0 ? ib : jb0 + tile - 1) * kMmaRows + r;
+                    const uint32_t bits = R < d ? g.rows[(size_t)R * g.S + kc] : 0u;
+                    expand_row_bits(ms.stage + tile * kMmaTileBytes, r, bits);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncthreads();
+                if (tid == 0) {
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t s0 = smem_addr(ms.stage);
+                    const uint64_t da = mma_desc(s0);
+                    const uint32_t acc = kc > k0 ? 1u : 0u;
+                    for (int t = 0; t < ng; ++t) {
+                        const uint64_t db = mma_desc(s0 + (uint32_t)(t + 1) * kMmaTileBytes);
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(
+                                ms.tmem + (uint32_t)(t * kMmaRows)),
+                            "l"(da), "l"(db), "r"(kMmaIdesc), "r"(acc), "r"(0u));
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     ms.mbar)
+                                 : "memory");
+                }
+                const bool ok = mbar_wait(ms.mbar, ms.phase);
+                ms.phase ^= 1u;
+                if (__syncthreads_or(!ok)) {
+                    if (tid == 0) atomicOr(err, 2u);
+                    return false;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            }
+            // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows of block ib), columns
+            // 16 c, 16 (c + kWarps / 4), ... of the ng accumulator tiles
+            const int q = warp & 3, i = ib * kMmaRows + q * 32 + lane;
+            const uint32_t *ri = g.rows + (size_t)min(i, d - 1) * g.S;
+            uint64_t sum = 0;
+            for (int col = (warp >> 2) * 16; col < ng * kMmaRows; col += (kWarps / 4) * 16) {
+                uint32_t v[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];\n"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15])
+                    : "r"(ms.tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                const int j0 = (jb0 + col / kMmaRows) * kMmaRows + col % kMmaRows;
+                const uint32_t m = (i < d && j0 < d) ? (ri[j0 >> 5] >> (j0 & 31)) & 0xFFFFu : 0u;
+#pragma unroll
+                for (int t = 0; t < 16; ++t) sum += (m >> t) & 1u ? v[t] : 0u;
+            }
+            a.cnt += sum;
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();  // every accumulator read before the next pass overwrites it
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        }
+    }
+    return true;
+}
+
 // warp reduction of the accumulator and one atomicAdd per counter into the job's row
 __device__ __forceinline__ void flush_acc(Acc &a, int K, uint64_t *row, uint64_t *phase_bytes) {
 #pragma unroll
@@ -590,10 +739,13 @@ __host__ __device__ __forceinline__ int block_logt(int dcap) {
 __host__ __device__ __forceinline__ size_t block_rows_words(int dcap) {
     return (size_t)((dcap + 31) & ~31) * 2 * ((size_t)((dcap + 63) / 64) | 1);
 }
-__host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads) {
+// the item rings, which the tensor-core count reuses as its operand stage of (mma_g + 1) tiles
+__host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads, int mma_g = 0) {
     const size_t dp = (size_t)((dcap + 31) & ~31);
     const size_t t = (size_t)1 << block_logt(dcap);
-    return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + block_rows_words(dcap) * 4 + (size_t)(threads / 32) * kRing * 4;
+    const size_t rings = (size_t)(threads / 32) * kRing * 4;
+    const size_t stage = mma_g > 0 ? (size_t)(mma_g + 1) * kMmaTileBytes : 0;
+    return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + block_rows_words(dcap) * 4 + (rings > stage ? rings : stage);
 }
 
 // Block tier: one block per start vertex; the list holds global start-vertex indices, heaviest
@@ -604,14 +756,19 @@ __host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads) {
 constexpr int kMidThreads = 256, kLargeAThreads = 512, kLargeThreads = 1024;
 constexpr int kMidMinBlocks = 5;
 constexpr int kLargeAMax = 640;
-template <bool STATS, int KMAX, int THREADS>
+// MMA: the build whose k = 4 jobs count on the tensor cores (mma_g accumulator tiles per pass); the
+// other build has no tensor-core code at all, so its CUDA-core count compiles as before
+template <bool STATS, int KMAX, int THREADS, bool MMA = false>
 __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREADS == kLargeAThreads ? 2 : kMidMinBlocks))
     clique_block_kernel(const BJob *__restrict__ jobs, int n_jobs, const uint32_t *__restrict__ list,
                                     const unsigned int *__restrict__ list_len, int dcap, unsigned long long *queue,
-                                    uint64_t *rows_out, uint64_t *phase_bytes) {
+                                    uint64_t *rows_out, uint64_t *phase_bytes, int mma_g, unsigned int *err) {
+    constexpr bool kMma = MMA && !STATS && THREADS != kMidThreads;
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_v0;
     __shared__ int s_job;
+    __shared__ __align__(8) uint64_t s_mbar;
+    __shared__ uint32_t s_tmem;
     const int dp = (dcap + 31) & ~31;
     const int logt = block_logt(dcap);
     const int T = 1 << logt;
@@ -625,6 +782,26 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
     const int warps = blockDim.x >> 5;
     const int wib = threadIdx.x >> 5;
     uint32_t *ring = g.rows + block_rows_words(dcap) + (size_t)wib * kRing;
+    const bool use_mma = kMma && mma_g > 0;
+    const uint32_t tmem_cols = mma_tmem_cols(mma_g);
+    MmaState ms{0, 0, 0, mma_g, reinterpret_cast<uint8_t *>(g.rows + block_rows_words(dcap))};  // stage: the rings
+    if (use_mma) {
+        if (wib == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                         "r"(tmem_cols));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+        }
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar)));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        ms.tmem = s_tmem;
+        ms.mbar = smem_addr(&s_mbar);
+    }
+    bool stalled = false;
     const unsigned int n_list = *list_len;
     Acc a = {0, 0, 0, 0};
     int cur_job = -1;
@@ -666,27 +843,47 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
         __syncthreads();
         build_rows(g, off, adj, wib, warps);
         __syncthreads();
-        row_extents(g, threadIdx.x, blockDim.x);
-        __syncthreads();
-        if (g.W <= 8) count_rows_units<STATS, KMAX>(g, jobs[j].k, off, wib, warps, a);
-        else count_rows<STATS, KMAX>(g, jobs[j].k, off, wib, warps, ring, a);
+        if (use_mma && jobs[j].k == 4) {
+            if (!count_rows_mma<THREADS>(g, ms, err, a)) {
+                stalled = true;
+                break;
+            }
+        } else {
+            row_extents(g, threadIdx.x, blockDim.x);
+            __syncthreads();
+            if (g.W <= 8) count_rows_units<STATS, KMAX>(g, jobs[j].k, off, wib, warps, a);
+            else count_rows<STATS, KMAX>(g, jobs[j].k, off, wib, warps, ring, a);
+        }
         __syncthreads();
     }
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
+    if (use_mma) {
+        // after a stall, give the outstanding MMAs one more bounded wait before the accumulators
+        // are released
+        if (stalled) mbar_wait(ms.mbar, ms.phase ^ 1u);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (wib == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(ms.tmem), "r"(tmem_cols));
+        }
+    }
 }
 
 using BlockKernel = void (*)(const BJob *, int, const uint32_t *, const unsigned int *, int, unsigned long long *,
-                             uint64_t *, uint64_t *);
+                             uint64_t *, uint64_t *, int, unsigned int *);
 template <int THREADS>
-BlockKernel block_kernel_of(bool stats, int kmax) {
+BlockKernel block_kernel_of(bool stats, int kmax, bool mma) {
+    if (mma && !stats && THREADS != kMidThreads)
+        return kmax == 5 ? clique_block_kernel<false, 5, THREADS, true> : clique_block_kernel<false, 4, THREADS, true>;
     return stats ? (kmax == 5 ? clique_block_kernel<true, 5, THREADS> : clique_block_kernel<true, 4, THREADS>)
                  : (kmax == 5 ? clique_block_kernel<false, 5, THREADS> : clique_block_kernel<false, 4, THREADS>);
 }
 // tier 0: mid, tier 1: lower large, tier 2: upper large
-BlockKernel block_kernel(bool stats, int kmax, int tier) {
-    return tier == 0   ? block_kernel_of<kMidThreads>(stats, kmax)
-           : tier == 1 ? block_kernel_of<kLargeAThreads>(stats, kmax)
-                       : block_kernel_of<kLargeThreads>(stats, kmax);
+BlockKernel block_kernel(bool stats, int kmax, int tier, bool mma = false) {
+    return tier == 0   ? block_kernel_of<kMidThreads>(stats, kmax, false)
+           : tier == 1 ? block_kernel_of<kLargeAThreads>(stats, kmax, mma)
+                       : block_kernel_of<kLargeThreads>(stats, kmax, mma);
 }
 // out-degrees (lo, hi] of block tier t
 __host__ __device__ __forceinline__ int tier_lo(int t, int warp_max) {
@@ -802,7 +999,7 @@ size_t bitmap_arena_bytes(const std::vector<BJob> &jobs, uint64_t list_cap) {
 }
 
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
-                          int warp_max, Arena *arena, BitmapLaunch *bl, cudaStream_t s) {
+                          int warp_max, bool tensor_cores, Arena *arena, BitmapLaunch *bl, cudaStream_t s) {
     BitmapLaunch L;
     L.warp_max = warp_max == 32 ? 32u : (uint32_t)kWarpMax;
     L.kmax = 4;
@@ -851,14 +1048,22 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     const int threads[BitmapLaunch::kTiers] = {kMidThreads, kLargeAThreads, kLargeThreads};
     for (int t = 0; t < BitmapLaunch::kTiers; ++t) {
         L.has_tier[t] = max_outdeg > (uint32_t)tier_lo(t, (int)L.warp_max);
-        const size_t smem = block_smem(dcaps[t], threads[t]);
-        const BlockKernel kern = block_kernel(stats, L.kmax, t);
-        // the attribute is per kernel, shared by every prepared launch: always allow the largest
-        // footprint so launches prepared earlier with more shared memory stay valid
-        KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)block_smem(kBlockMax, 1024)));
+        // large tiers: the most accumulator tiles per pass whose tensor memory fits every block
+        // resident on an SM at once (512 columns per SM; an allocation would otherwise wait)
+        int g = (t > 0 && tensor_cores && !stats) ? (t == 2 ? kMmaMaxTiles : 2) : 0;
+        size_t smem = 0;
         int per_sm = 0;
-        KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
+        BlockKernel kern = nullptr;
+        for (;; --g) {
+            kern = block_kernel(stats, L.kmax, t, g > 0);
+            // the attribute is per kernel, shared by every prepared launch: always allow the largest
+            // footprint so launches prepared earlier with more shared memory stay valid
+            KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)block_smem(kBlockMax, 1024, kMmaMaxTiles)));
+            smem = block_smem(dcaps[t], threads[t], g);
+            KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
+            if (g == 0 || per_sm * (int)mma_tmem_cols(g) <= 512) break;
+        }
         if (per_sm < 1) {
             set_error("bitmap block kernel does not fit an SM (%d threads, %zu bytes of shared memory)", threads[t], smem);
             return KHZ_ERR_CUDA;
@@ -867,12 +1072,14 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
         L.block_threads[t] = threads[t];
         L.block_grid[t] = L.sms * std::max(per_sm, 1);
         L.block_dcap[t] = dcaps[t];
+        L.block_mma_g[t] = g;
     }
     *bl = L;
     return KHZ_OK;
 }
 
-khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls) {
+khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls,
+                          unsigned int *d_err) {
     if (L.n_jobs == 0 || L.n_total == 0) return KHZ_OK;
     auto pb = [&](int phase) -> uint64_t * { return ls && ls->d_phase_bytes ? ls->d_phase_bytes + phase : nullptr; };
     auto mark = [&](int phase, bool begin) {
@@ -916,9 +1123,10 @@ khz_status bitmap_enqueue(const BitmapLaunch &L, uint64_t *d_rows, cudaStream_t 
         if (!L.has_tier[t]) continue;
         const int phase = t == 0 ? 1 : 2;
         if (t != 2 || !L.has_tier[1]) mark(phase, true);
-        const BlockKernel bk = block_kernel(L.stats, L.kmax, t);
+        const BlockKernel bk = block_kernel(L.stats, L.kmax, t, L.block_mma_g[t] > 0);
         bk<<<L.block_grid[t], L.block_threads[t], L.block_smem[t], s>>>(
-            L.d_jobs, L.n_jobs, L.lists[t], L.cnt + kCntLen + t, L.block_dcap[t], &L.queues[1 + t], d_rows, pb(phase));
+            L.d_jobs, L.n_jobs, L.lists[t], L.cnt + kCntLen + t, L.block_dcap[t], &L.queues[1 + t], d_rows, pb(phase),
+            L.block_mma_g[t], d_err);
         KHZ_CUDA(cudaGetLastError());
         if (t == 0 || t == last_large) mark(phase, false);
         if (ls) ls->launches += 1;

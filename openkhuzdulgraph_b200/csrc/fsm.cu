@@ -46,6 +46,8 @@ struct FsmArgs {
     const uint8_t *pre2;    // L^3: some candidate's first three labels
     uint32_t *domains;      // [candidate][position][words]
     uint32_t words;         // ceil(n / 32)
+    uint64_t m;             // CSR entries (the (v0, v1) pairs)
+    unsigned long long *queue;  // pair claims of one launch (zeroed before it)
 };
 
 __device__ __forceinline__ void mark(const FsmArgs &a, int cand, int pos, uint32_t v) {
@@ -63,71 +65,100 @@ __device__ __forceinline__ bool contains(const uint32_t *list, uint32_t len, uin
     return p < len && __ldg(list + p) == x;
 }
 
-// One warp per start vertex v0; the embeddings enumerated are exactly those the app's apply()
-// inserts into its pattern domain with enable = true (three_fsm.cc:53-262):
+// The embeddings enumerated are exactly those the app's apply() inserts into its pattern domain
+// with enable = true (three_fsm.cc:53-262):
 //   edge        v1 in N(v0)
 //   wedge       v1 in N(v0); v2 in N(v0), v2 != v1
 //   triangle    v1 in N(v0); v2 in N(v0) n N(v1)
 //   four-chain  v1 in N(v0); v2 in N(v0), v2 != v1; v3 in N(v1), v3 != v0, v3 != v2
 //   three-star  v1 in N(v0); v2 in N(v1), v2 != v0; v3 in N(v1), v3 != v0, v3 != v2
+// The edge template takes one warp per v0.  The others take one warp per (v0, v1) pair: pairs are
+// CSR entries, claimed in chunks from a counter, so a hub's pairs spread over many warps instead of
+// one warp walking d(v0)^2 d(v1) / 32 steps alone.
+
+// the embeddings that extend the pair (v0, v1 = N(v0)[i1]); lanes take the last vertex
+template <int T>
+__device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t v1) {
+    const unsigned lane = lane_id();
+    const uint32_t L = a.L;
+    const uint32_t l0 = __ldg(a.labels + v0);
+    const uint32_t l1 = __ldg(a.labels + v1);
+    if (!a.pre1[l0 * L + l1]) return;
+    const uint32_t *n0 = a.adj + a.off[v0];
+    const uint32_t d0 = (uint32_t)(a.off[v0 + 1] - a.off[v0]);
+    const uint32_t base01 = (l0 * L + l1) * L;
+    const uint32_t *n1 = a.adj + a.off[v1];
+    const uint32_t d1 = (uint32_t)(a.off[v1 + 1] - a.off[v1]);
+    if constexpr (T == kWedge || T == kTriangle) {
+        for (uint32_t i = lane; i < d0; i += 32) {
+            const uint32_t v2 = __ldg(n0 + i);
+            if (v2 == v1) continue;
+            const int c = a.table[base01 + __ldg(a.labels + v2)];
+            if (c < 0) continue;
+            if (T == kTriangle && !contains(n1, d1, v2)) continue;
+            const uint32_t v[3] = {v0, v1, v2};
+            mark_all(a, c, 3, v);
+        }
+    } else {
+        // four-chain: v2 from N(v0); three-star: v2 from N(v1)
+        const uint32_t *n2s = T == kFourChain ? n0 : n1;
+        const uint32_t d2s = T == kFourChain ? d0 : d1;
+        for (uint32_t i2 = 0; i2 < d2s; ++i2) {
+            const uint32_t v2 = __ldg(n2s + i2);
+            if (T == kFourChain ? v2 == v1 : v2 == v0) continue;
+            const uint32_t l2 = __ldg(a.labels + v2);
+            if (!a.pre2[base01 + l2]) continue;
+            const uint32_t base012 = (base01 + l2) * L;
+            for (uint32_t i = lane; i < d1; i += 32) {
+                const uint32_t v3 = __ldg(n1 + i);
+                if (v3 == v0 || v3 == v2) continue;
+                const int c = a.table[base012 + __ldg(a.labels + v3)];
+                if (c < 0) continue;
+                const uint32_t v[4] = {v0, v1, v2, v3};
+                mark_all(a, c, 4, v);
+            }
+        }
+    }
+}
+
 template <int T>
 __global__ void __launch_bounds__(256) fsm_domain_kernel(FsmArgs a) {
     const unsigned lane = lane_id();
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t L = a.L;
-    for (uint32_t v0 = warp; v0 < a.n; v0 += nwarps) {
-        const uint32_t l0 = __ldg(a.labels + v0);
-        const uint32_t *n0 = a.adj + a.off[v0];
-        const uint32_t d0 = (uint32_t)(a.off[v0 + 1] - a.off[v0]);
-        if constexpr (T == kEdge) {
+    if constexpr (T == kEdge) {
+        const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+        for (uint32_t v0 = warp; v0 < a.n; v0 += nwarps) {
+            const uint32_t l0 = __ldg(a.labels + v0);
+            const uint32_t *n0 = a.adj + a.off[v0];
+            const uint32_t d0 = (uint32_t)(a.off[v0 + 1] - a.off[v0]);
             for (uint32_t i = lane; i < d0; i += 32) {
                 const uint32_t v1 = __ldg(n0 + i);
-                const int c = a.table[l0 * L + __ldg(a.labels + v1)];
+                const int c = a.table[l0 * a.L + __ldg(a.labels + v1)];
                 if (c >= 0) {
                     const uint32_t v[2] = {v0, v1};
                     mark_all(a, c, 2, v);
                 }
             }
-        } else {
-        for (uint32_t i1 = 0; i1 < d0; ++i1) {
-            const uint32_t v1 = __ldg(n0 + i1);
-            const uint32_t l1 = __ldg(a.labels + v1);
-            if (!a.pre1[l0 * L + l1]) continue;
-            const uint32_t base01 = (l0 * L + l1) * L;
-            const uint32_t *n1 = a.adj + a.off[v1];
-            const uint32_t d1 = (uint32_t)(a.off[v1 + 1] - a.off[v1]);
-            if (T == kWedge || T == kTriangle) {
-                for (uint32_t i = lane; i < d0; i += 32) {
-                    const uint32_t v2 = __ldg(n0 + i);
-                    if (v2 == v1) continue;
-                    const int c = a.table[base01 + __ldg(a.labels + v2)];
-                    if (c < 0) continue;
-                    if (T == kTriangle && !contains(n1, d1, v2)) continue;
-                    const uint32_t v[3] = {v0, v1, v2};
-                    mark_all(a, c, 3, v);
-                }
-                continue;
-            }
-            // four-chain: v2 from N(v0); three-star: v2 from N(v1)
-            const uint32_t *n2s = T == kFourChain ? n0 : n1;
-            const uint32_t d2s = T == kFourChain ? d0 : d1;
-            for (uint32_t i2 = 0; i2 < d2s; ++i2) {
-                const uint32_t v2 = __ldg(n2s + i2);
-                if (T == kFourChain ? v2 == v1 : v2 == v0) continue;
-                const uint32_t l2 = __ldg(a.labels + v2);
-                if (!a.pre2[base01 + l2]) continue;
-                const uint32_t base012 = (base01 + l2) * L;
-                for (uint32_t i = lane; i < d1; i += 32) {
-                    const uint32_t v3 = __ldg(n1 + i);
-                    if (v3 == v0 || v3 == v2) continue;
-                    const int c = a.table[base012 + __ldg(a.labels + v3)];
-                    if (c < 0) continue;
-                    const uint32_t v[4] = {v0, v1, v2, v3};
-                    mark_all(a, c, 4, v);
-                }
-            }
         }
+    } else {
+        constexpr uint64_t kChunk = 8;
+        while (true) {
+            unsigned long long e0 = 0;
+            if (lane == 0) e0 = atomicAdd(a.queue, (unsigned long long)kChunk);
+            e0 = __shfl_sync(kFull, e0, 0);
+            if (e0 >= a.m) break;
+            const uint64_t e1 = min((uint64_t)a.m, (uint64_t)e0 + kChunk);
+            // v0 of entry e0: the largest v with off[v] <= e0 (its list holds e0, as e0 < m)
+            uint32_t lo = 0, hi = a.n;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (a.off[mid] <= e0) lo = mid; else hi = mid - 1;
+            }
+            uint32_t v0 = lo;
+            for (uint64_t e = e0; e < e1; ++e) {
+                while (a.off[v0 + 1] <= e) ++v0;
+                fsm_pair<T>(a, v0, __ldg(a.adj + e));
+            }
         }
     }
 }
@@ -263,16 +294,19 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     int32_t *d_table = nullptr;
     uint8_t *d_pre = nullptr;
     uint32_t *d_dom = nullptr, *d_sizes = nullptr;
+    unsigned long long *d_queue = nullptr;
     auto release = [&]() {
         cudaFree(d_table);
         cudaFree(d_pre);
         cudaFree(d_dom);
         cudaFree(d_sizes);
+        cudaFree(d_queue);
     };
     cudaError_t e = cudaMalloc(&d_table, sizeof(int32_t) * tsize);
     if (e == cudaSuccess) e = cudaMalloc(&d_pre, (size_t)L * L + (size_t)L * L * L);
     if (e == cudaSuccess) e = cudaMalloc(&d_dom, per_cand * group_max);
     if (e == cudaSuccess) e = cudaMalloc(&d_sizes, sizeof(uint32_t) * 4 * group_max);
+    if (e == cudaSuccess) e = cudaMalloc(&d_queue, sizeof(unsigned long long));
     if (e != cudaSuccess) {
         cudaGetLastError();
         release();
@@ -316,7 +350,12 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
                 release();
                 return cuda_fail(cudaGetLastError(), "3-FSM tables");
             }
-            FsmArgs a{gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_table, d_pre, d_pre + (size_t)L * L, d_dom, words};
+            if (cudaMemset(d_queue, 0, sizeof(unsigned long long)) != cudaSuccess) {
+                release();
+                return cuda_fail(cudaGetLastError(), "3-FSM pair counter");
+            }
+            FsmArgs a{gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_table, d_pre, d_pre + (size_t)L * L, d_dom, words,
+                      gi.num_entries, d_queue};
             switch (t) {
                 case kEdge: fsm_domain_kernel<kEdge><<<grid, 256>>>(a); break;
                 case kWedge: fsm_domain_kernel<kWedge><<<grid, 256>>>(a); break;

@@ -630,7 +630,9 @@ khz_status build_plan(khz_ctx *ctx, const khz_job *jobs, int n, cudaStream_t s, 
     KHZ_CUDA(cudaMemcpyAsync(P->d_mult, mult.data(), sizeof(uint32_t) * mult.size(), cudaMemcpyHostToDevice, s));
     KHZ_CUDA(cudaMemcpyAsync(P->d_extadd, ext_add.data(), sizeof(uint64_t) * total, cudaMemcpyHostToDevice, s));
     khz_status st = KHZ_OK;
-    if (P->has_bitmap) st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, warp_max, &P->arena, &P->bl, s);
+    if (P->has_bitmap)
+        st = bitmap_prepare(bjobs, bmax, list_cap, P->stats, warp_max, ctx->cfg.bitmap_tensor_cores > 0, &P->arena,
+                            &P->bl, s);
     if (st) return st;
     if (!motif_jobs.empty()) st = motif_prepare(motif_jobs, &P->arena, &P->ml, s);
     if (st) return st;
@@ -669,7 +671,7 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
     if (ls) ls->d_phase_bytes = P->d_phase_bytes;
     if (ev_begin) KHZ_CUDA(cudaEventRecord(ev_begin, s));
     khz_status st = KHZ_OK;
-    if (P->has_bitmap) st = bitmap_enqueue(P->bl, P->d_raw, s, ls);
+    if (P->has_bitmap) st = bitmap_enqueue(P->bl, P->d_raw, s, ls, P->d_bad);
     if (st) return st;
     if (P->has_dfs) st = dfs_enqueue(P->dl, P->d_raw, s, ls, P->own_scratch ? nullptr : shared_slots);
     if (st) return st;
@@ -693,6 +695,21 @@ khz_status enqueue_plan(BatchPlan *P, cudaStream_t s, LaunchStats *ls, cudaEvent
     return KHZ_OK;
 }
 
+// the status a launch's device flag word reports: bit 1 a count not divisible by the pattern's
+// multiplicity (finalize), bit 2 a tensor-core pass of the bitmap engine that did not complete
+// within its poll limit (the counts are then incomplete)
+khz_status launch_flags_status(unsigned int flags) {
+    if (flags & 2u) {
+        set_error("a tensor-core counting pass did not complete within its wait limit; the counts are incomplete");
+        return KHZ_ERR_CUDA;
+    }
+    if (flags) {
+        set_error("raw count not divisible by the pattern multiplicity (input is not an undirected graph)");
+        return KHZ_ERR_MULTIPLICITY;
+    }
+    return KHZ_OK;
+}
+
 // copy the finalized rows to pinned memory (the plan's, or `host` for shared-scratch plans)
 // and wait for them
 khz_status read_plan(BatchPlan *P, cudaStream_t s, uint64_t *host = nullptr) {
@@ -701,11 +718,7 @@ khz_status read_plan(BatchPlan *P, cudaStream_t s, uint64_t *host = nullptr) {
     KHZ_CUDA(cudaMemcpyAsync(P->h_final, P->d_final, sizeof(uint64_t) * words, cudaMemcpyDeviceToHost, s));
     KHZ_CUDA(cudaMemcpyAsync(P->h_final + words, P->d_bad, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     KHZ_CUDA(cudaStreamSynchronize(s));
-    if (*(const unsigned int *)(P->h_final + words)) {
-        set_error("raw count not divisible by the pattern multiplicity (input is not an undirected graph)");
-        return KHZ_ERR_MULTIPLICITY;
-    }
-    return KHZ_OK;
+    return launch_flags_status(*(const unsigned int *)(P->h_final + words));
 }
 
 khz_status fill_stats(khz_ctx *ctx, BatchPlan *P, const LaunchStats &ls, bool timed, khz_stats *stats) {
@@ -847,7 +860,7 @@ bool serve_reap(khz_server *sv) {
         khz_status st = KHZ_OK;
         if (q != cudaSuccess) st = cuda_fail(q, "serving slot");
         const size_t words = (size_t)kRowWords * sl.reqs.size();
-        if (st == KHZ_OK && *(const unsigned int *)(sl.h_rows + words)) st = KHZ_ERR_MULTIPLICITY;
+        if (st == KHZ_OK) st = launch_flags_status(*(const unsigned int *)(sl.h_rows + words));
         {
             std::lock_guard<std::mutex> lk(sv->mu);
             for (size_t i = 0; i < sl.reqs.size(); ++i) {

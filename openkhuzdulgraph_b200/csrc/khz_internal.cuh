@@ -163,6 +163,8 @@ struct BitmapLaunch {
     int sms = 0;
     size_t block_smem[kTiers] = {};
     int block_threads[kTiers] = {}, block_grid[kTiers] = {}, block_dcap[kTiers] = {};
+    // tensor-memory accumulator tiles per pass of the large tiers' 4-clique count (0: CUDA cores)
+    int block_mma_g[kTiers] = {};
     std::vector<BJob> hubs;  // jobs with a hub triangle to build before the counting kernels
 };
 
@@ -326,9 +328,12 @@ khz_status wedge_enqueue(const WedgeLaunch &wl, uint64_t *d_rows, cudaStream_t s
 uint32_t bitmap_hub_rows(int cfg_rows, uint32_t n, uint64_t m);
 size_t bitmap_hub_bytes(uint32_t rows);
 size_t bitmap_arena_bytes(const std::vector<BJob> &jobs, uint64_t list_cap);
+// tensor_cores: the large tiers count 4-cliques as a masked 0/1 matrix product on the tensor cores
 khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, uint64_t list_cap, bool stats,
-                          int warp_max, Arena *arena, BitmapLaunch *bl, cudaStream_t s);
-khz_status bitmap_enqueue(const BitmapLaunch &bl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls);
+                          int warp_max, bool tensor_cores, Arena *arena, BitmapLaunch *bl, cudaStream_t s);
+// d_err: bit 2 is set if a tensor-core pass did not complete within its poll limit
+khz_status bitmap_enqueue(const BitmapLaunch &bl, uint64_t *d_rows, cudaStream_t s, LaunchStats *ls,
+                          unsigned int *d_err);
 uint32_t bitmap_block_max_degree();
 
 }  // namespace khz

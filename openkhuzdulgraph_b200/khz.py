@@ -87,7 +87,7 @@ class Config(ctypes.Structure):
                 ("dfs_warps_per_sm", ctypes.c_int32), ("dfs_chunk", ctypes.c_int32),
                 ("bitmap_warp_max", ctypes.c_int32), ("bitmap_block_warps", ctypes.c_int32),
                 ("bitmap_hub_rows", ctypes.c_int32), ("device_mem_limit_mib", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 8)]
+                ("bitmap_tensor_cores", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7)]
 
 
 class ServerStats(ctypes.Structure):

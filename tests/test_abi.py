@@ -57,7 +57,7 @@ def test_config_layout_is_fixed():
     import ctypes
     assert ctypes.sizeof(khz.Config) == 64
     assert khz.Config.bitmap_hub_rows.offset == 24 and khz.Config.device_mem_limit_mib.offset == 28
-    assert khz.Config.reserved.offset == 32
+    assert khz.Config.bitmap_tensor_cores.offset == 32 and khz.Config.reserved.offset == 36
 
 
 def test_graph_info_layout():

@@ -333,6 +333,43 @@ def test_bitmap_large_tier_matches_oracle(khz_ctx):
         og.free()
 
 
+@pytest.mark.timeout(900, method="thread")
+def test_tensor_core_four_clique_matches(khz_ctx):
+    """bitmap_tensor_cores = 1: the large tiers count 4-cliques as a masked 0/1 matrix product on the
+    tensor cores.  Dense ER (out-degrees up to ~700, both large tiers, row blocks of 128 with ragged
+    ends) against the oracle; an R-MAT s18 against the CUDA-core count; 5-clique and triangle jobs
+    of the same launches stay on the CUDA cores and keep their counts."""
+    from openkhuzdulgraph_b200 import khz
+    canon, n = orc.er(1500, 250000, seed=5)
+    sym = orc.symmetrize(canon)
+    off, adj = orc.csr(sym, n)
+    ooff, oadj, _ = orc.orient(off, adj)
+    og = khz_ctx.graph_from_edges(sym, n, orient=True)
+    rm = khz_ctx.generate_rmat(18, 16, seed=1)
+    rog = rm.orient()
+    try:
+        khz_ctx.set_config(engine=khz.ENGINE_BITMAP, bitmap_tensor_cores=1)
+        got, st = khz_ctx.count(og, "kautomine_four_clique")
+        exp, ext, _ = orc.count("kautomine_four_clique", ooff, oadj)
+        assert got == exp and st.num_extensions == ext
+        assert st.phase_launches[2] >= 1
+        tc = {app: khz_ctx.count(rog, app) for app in ["kautomine_four_clique", "kgraphpi_four_clique",
+                                                        "kautomine_five_clique", "kautomine_triangle"]}
+        batch, exts, _ = khz_ctx.count_batch([(rog, "kautomine_five_clique"), (rog, "kautomine_four_clique"),
+                                             (og, "kgraphpi_four_clique")])
+        khz_ctx.set_config(engine=khz.ENGINE_BITMAP, bitmap_tensor_cores=0)
+        for app, (c, s) in tc.items():
+            c0, s0 = khz_ctx.count(rog, app)
+            assert c == c0 and s.num_extensions == s0.num_extensions, app
+        assert batch[1] == tc["kautomine_four_clique"][0] and batch[2] == exp
+        assert batch[0] == tc["kautomine_five_clique"][0]
+    finally:
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO, bitmap_tensor_cores=0)
+        og.free()
+        rog.free()
+        rm.free()
+
+
 @pytest.mark.parametrize("hub_rows", [64, 992, 1 << 30])
 def test_hub_triangle_matches_oracle(graphs, khz_ctx, hub_rows):
     """Rows of hub vertices read from the hub adjacency triangle (here forced on small graphs, up
