@@ -136,17 +136,20 @@ constexpr int kScanUnroll = 4;
 
 // Row i of a hub vertex from the triangle: lane l tests candidate j = 32 w + l (j > i), and the
 // ballot over the warp is word w of the row, stored whole (the calling warp owns the row).
-constexpr int kHubUnroll = 2;
+// U words per step (their loads in flight together): 4 in the large tiers, whose rows are long
+// and almost all hub rows; 2 elsewhere.  (Lanes outside (i, d) skip their load: a variant that
+// loaded on every lane and masked the ballot instead measured 12 % slower.)
+template <int U>
 __device__ __forceinline__ void hub_row(const Local &g, int i) {
     const int lane = (int)lane_id();
     const uint32_t h = g.c[i] - g.hub_base;
     const uint32_t *hrow = g.hub + hub_row_offset(h, g.hub_wh);
     const uint32_t wb = (h + 1) >> 5;
     uint32_t *row = g.rows + (size_t)i * g.S;
-    for (int w = (i + 1) >> 5; w < g.W; w += kHubUnroll) {
-        bool bit[kHubUnroll];
+    for (int w = (i + 1) >> 5; w < g.W; w += U) {
+        bool bit[U];
 #pragma unroll
-        for (int u = 0; u < kHubUnroll; ++u) {
+        for (int u = 0; u < U; ++u) {
             const int j = ((w + u) << 5) + lane;
             bit[u] = false;
             if (j > i && j < g.d) {
@@ -155,13 +158,14 @@ __device__ __forceinline__ void hub_row(const Local &g, int i) {
             }
         }
 #pragma unroll
-        for (int u = 0; u < kHubUnroll; ++u) {
+        for (int u = 0; u < U; ++u) {
             const unsigned m = __ballot_sync(kFull, bit[u]);
             if (lane == 0 && w + u < g.W) row[w + u] = m;
         }
     }
 }
 
+template <int U = 2>
 __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, const uint32_t *__restrict__ adj,
                            int row_begin, int row_step) {
     const unsigned lane = lane_id();
@@ -190,7 +194,7 @@ __device__ void build_rows(const Local &g, const uint64_t *__restrict__ off, con
         for (int r = 0; r < nrows; ++r) {
             const int i = i0 + r * row_step;
             if (g.hub && g.c[i] >= g.hub_base) {
-                hub_row(g, i);
+                hub_row<U>(g, i);
                 continue;
             }
             const uint32_t sp = sp_next;
@@ -521,14 +525,30 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
 }
 
 struct MmaState {
-    uint32_t tmem;    // tensor-memory base of the accumulators (G x 128 columns)
-    uint32_t mbar;    // shared address of the MMA-completion mbarrier
-    uint32_t phase;   // parity of the next completion
-    int G;            // accumulator tiles per pass
-    uint8_t *stage;   // (G + 1) operand tiles
+    uint32_t tmem;       // tensor-memory base of the accumulators (G x 128 columns)
+    uint32_t mbar[2];    // shared addresses of the two stages' MMA-completion mbarriers
+    uint32_t phase[2];   // parity of each barrier's next completion
+    uint32_t pending[2]; // 1 while a commit to the barrier has not been waited for
+    int G;               // accumulator tiles per pass
+    uint8_t *stage;      // two stages of (G + 1) operand tiles each
 };
 
-// 4-clique count of one start vertex on the tensor cores.  Returns false (after recording the
+// wait for the MMAs last committed to stage st's barrier (block-uniform); false, with the stall
+// recorded and the commit left pending, after the poll limit
+__device__ __forceinline__ bool mma_stage_wait(MmaState &ms, int st, unsigned int *err) {
+    const bool ok = mbar_wait(ms.mbar[st], ms.phase[st]);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(err, 2u);
+        return false;
+    }
+    ms.phase[st] ^= 1u;
+    ms.pending[st] = 0;
+    return true;
+}
+
+// 4-clique count of one start vertex on the tensor cores.  The 32-column steps of a pass alternate
+// between two operand stages: step s expands into stage s & 1 while the MMAs of step s - 1 run, and
+// waits only for step s - 2 (the last reader of that stage).  Returns false (after recording the
 // stall in *err) if an MMA completion was not seen within the poll limit; the caller then stops.
 template <int THREADS>
 __device__ bool count_rows_mma(const Local &g, MmaState &ms, unsigned int *err, Acc &a) {
@@ -544,24 +564,28 @@ __device__ bool count_rows_mma(const Local &g, MmaState &ms, unsigned int *err, 
     }
     const int nb = (d + kMmaRows - 1) / kMmaRows;
     const int kw = g.W;  // 32-column steps
+    const uint32_t stage_bytes = (uint32_t)(ms.G + 1) * kMmaTileBytes;
     for (int ib = 0; ib < nb; ++ib) {
         for (int jb0 = ib; jb0 < nb; jb0 += ms.G) {
             const int ng = min(ms.G, nb - jb0);
             const int k0 = jb0 * (kMmaRows / 32);
             for (int kc = k0; kc < kw; ++kc) {
-                // stage: tile 0 = rows of block ib, tile 1 + t = rows of block jb0 + t
+                const int st = (kc - k0) & 1;
+                if (ms.pending[st] && !mma_stage_wait(ms, st, err)) return false;
+                // stage st: tile 0 = rows of block ib, tile 1 + t = rows of block jb0 + t
+                uint8_t *stage = ms.stage + st * stage_bytes;
                 for (int task = tid; task < (ng + 1) * kMmaRows; task += THREADS) {
                     const int tile = task / kMmaRows, r = task % kMmaRows;
                     const int R = (tile == 0 ? ib : jb0 + tile - 1) * kMmaRows + r;
                     const uint32_t bits = R < d ? g.rows[(size_t)R * g.S + kc] : 0u;
-                    expand_row_bits(ms.stage + tile * kMmaTileBytes, r, bits);
+                    expand_row_bits(stage + tile * kMmaTileBytes, r, bits);
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncthreads();
                 if (tid == 0) {
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t s0 = smem_addr(ms.stage);
+                    const uint32_t s0 = smem_addr(stage);
                     const uint64_t da = mma_desc(s0);
                     const uint32_t acc = kc > k0 ? 1u : 0u;
                     for (int t = 0; t < ng; ++t) {
@@ -573,17 +597,15 @@ __device__ bool count_rows_mma(const Local &g, MmaState &ms, unsigned int *err, 
                             "l"(da), "l"(db), "r"(kMmaIdesc), "r"(acc), "r"(0u));
                     }
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                     ms.mbar)
+                                     ms.mbar[st])
                                  : "memory");
                 }
-                const bool ok = mbar_wait(ms.mbar, ms.phase);
-                ms.phase ^= 1u;
-                if (__syncthreads_or(!ok)) {
-                    if (tid == 0) atomicOr(err, 2u);
-                    return false;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                ms.pending[st] = 1;
             }
+            // the pass's last one or two steps are still outstanding, one per stage
+            for (int st = 0; st < 2; ++st)
+                if (ms.pending[st] && !mma_stage_wait(ms, st, err)) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows of block ib), columns
             // 16 c, 16 (c + kWarps / 4), ... of the ng accumulator tiles
             const int q = warp & 3, i = ib * kMmaRows + q * 32 + lane;
@@ -739,12 +761,12 @@ __host__ __device__ __forceinline__ int block_logt(int dcap) {
 __host__ __device__ __forceinline__ size_t block_rows_words(int dcap) {
     return (size_t)((dcap + 31) & ~31) * 2 * ((size_t)((dcap + 63) / 64) | 1);
 }
-// the item rings, which the tensor-core count reuses as its operand stage of (mma_g + 1) tiles
+// the item rings, which the tensor-core count reuses for its two operand stages of (mma_g + 1) tiles
 __host__ __device__ __forceinline__ size_t block_smem(int dcap, int threads, int mma_g = 0) {
     const size_t dp = (size_t)((dcap + 31) & ~31);
     const size_t t = (size_t)1 << block_logt(dcap);
     const size_t rings = (size_t)(threads / 32) * kRing * 4;
-    const size_t stage = mma_g > 0 ? (size_t)(mma_g + 1) * kMmaTileBytes : 0;
+    const size_t stage = mma_g > 0 ? (size_t)2 * (mma_g + 1) * kMmaTileBytes : 0;
     return dp * 4 + t * 4 + t * 2 + dp * 2 * 2 + block_rows_words(dcap) * 4 + (rings > stage ? rings : stage);
 }
 
@@ -767,7 +789,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_v0;
     __shared__ int s_job;
-    __shared__ __align__(8) uint64_t s_mbar;
+    __shared__ __align__(8) uint64_t s_mbar[2];
     __shared__ uint32_t s_tmem;
     const int dp = (dcap + 31) & ~31;
     const int logt = block_logt(dcap);
@@ -784,7 +806,8 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
     uint32_t *ring = g.rows + block_rows_words(dcap) + (size_t)wib * kRing;
     const bool use_mma = kMma && mma_g > 0;
     const uint32_t tmem_cols = mma_tmem_cols(mma_g);
-    MmaState ms{0, 0, 0, mma_g, reinterpret_cast<uint8_t *>(g.rows + block_rows_words(dcap))};  // stage: the rings
+    MmaState ms{0, {0, 0}, {0, 0}, {0, 0}, mma_g,
+                reinterpret_cast<uint8_t *>(g.rows + block_rows_words(dcap))};  // stages: over the rings
     if (use_mma) {
         if (wib == 0) {
             asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
@@ -792,14 +815,16 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
             asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
         }
         if (threadIdx.x == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar)));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar[0])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar[1])));
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         ms.tmem = s_tmem;
-        ms.mbar = smem_addr(&s_mbar);
+        ms.mbar[0] = smem_addr(&s_mbar[0]);
+        ms.mbar[1] = smem_addr(&s_mbar[1]);
     }
     bool stalled = false;
     const unsigned int n_list = *list_len;
@@ -841,7 +866,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
         __syncthreads();
         hash_insert(g, threadIdx.x, blockDim.x);
         __syncthreads();
-        build_rows(g, off, adj, wib, warps);
+        build_rows<THREADS == kMidThreads ? 2 : 4>(g, off, adj, wib, warps);
         __syncthreads();
         if (use_mma && jobs[j].k == 4) {
             if (!count_rows_mma<THREADS>(g, ms, err, a)) {
@@ -859,8 +884,10 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
     if (cur_job >= 0) flush_acc(a, jobs[cur_job].k, row_of(rows_out, jobs[cur_job]), phase_bytes);
     if (use_mma) {
         // after a stall, give the outstanding MMAs one more bounded wait before the accumulators
-        // are released
-        if (stalled) mbar_wait(ms.mbar, ms.phase ^ 1u);
+        // are released (a completed phase makes the wait return at once)
+        if (stalled)
+            for (int st = 0; st < 2; ++st)
+                if (ms.pending[st]) mbar_wait(ms.mbar[st], ms.phase[st]);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         if (wib == 0) {
@@ -1041,6 +1068,9 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
     int dev = 0;
     KHZ_CUDA(cudaGetDevice(&dev));
     KHZ_CUDA(cudaDeviceGetAttribute(&L.sms, cudaDevAttrMultiProcessorCount, dev));
+    int optin = 0;
+    KHZ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t smem_optin = (size_t)optin;
     // each tier's shared memory is sized for the largest degree it serves in this launch
     const int dcaps[BitmapLaunch::kTiers] = {
         kMidMax, (int)std::min<uint32_t>((uint32_t)kLargeAMax, std::max<uint32_t>(max_outdeg, kMidMax + 1)),
@@ -1057,12 +1087,18 @@ khz_status bitmap_prepare(const std::vector<BJob> &jobs, uint32_t max_outdeg, ui
         for (;; --g) {
             kern = block_kernel(stats, L.kmax, t, g > 0);
             // the attribute is per kernel, shared by every prepared launch: always allow the largest
-            // footprint so launches prepared earlier with more shared memory stay valid
+            // footprint (up to the device's opt-in limit) so launches prepared earlier with more
+            // shared memory stay valid
+            cudaFuncAttributes fa;
+            KHZ_CUDA(cudaFuncGetAttributes(&fa, kern));
+            const size_t dyn_max = smem_optin - std::min(smem_optin, (size_t)fa.sharedSizeBytes);  // less static
             KHZ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)block_smem(kBlockMax, 1024, kMmaMaxTiles)));
+                                          (int)std::min(block_smem(kBlockMax, 1024, kMmaMaxTiles), dyn_max)));
             smem = block_smem(dcaps[t], threads[t], g);
-            KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
-            if (g == 0 || per_sm * (int)mma_tmem_cols(g) <= 512) break;
+            per_sm = 0;
+            if (smem <= dyn_max)
+                KHZ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads[t], smem));
+            if (g == 0 || (per_sm >= 1 && per_sm * (int)mma_tmem_cols(g) <= 512)) break;
         }
         if (per_sm < 1) {
             set_error("bitmap block kernel does not fit an SM (%d threads, %zu bytes of shared memory)", threads[t], smem);
