@@ -302,7 +302,7 @@ khz_status khz_batch_destroy(khz_batch *batch);
 /* ---- autotuner ---------------------------------------------------------------------- */
 /* Times the given jobs (a representative sample of the workload) under candidate settings —
  * engine (the bitmap / wedge / identity engines vs the DFS engine's warp-cooperative binary-search
- * probes), DFS warps per SM {8, 16, 32}, DFS units per grab {2, 8, 32}, bitmap warp-tier degree
+ * probes), DFS warps per SM {8, 16, 24}, DFS units per grab {2, 8, 32}, bitmap warp-tier degree
  * threshold {32, 64}, hub-triangle rows {auto, none, 8192} — by coordinate descent (two passes,
  * best of `reps` each), checks that every
  * candidate produces the same counts, and installs the fastest in the context. */

@@ -529,5 +529,5 @@ def test_autotuner_keeps_counts_and_installs_settings(graphs, khz_ctx):
         assert cfg.engine == rep["engine"] and cfg.dfs_chunk == rep["dfs_chunk"]
         assert [khz_ctx.count(g, app)[0] for g, app in jobs] == expect
     finally:
-        khz_ctx.set_config(engine=khz.ENGINE_AUTO, dfs_warps_per_sm=16, dfs_chunk=8, bitmap_warp_max=64,
-                           bitmap_hub_rows=0)
+        khz_ctx.set_config(engine=khz.ENGINE_AUTO, dfs_warps_per_sm=0, dfs_chunk=0, bitmap_warp_max=64,
+                           bitmap_hub_rows=0)  # 0: the defaults
