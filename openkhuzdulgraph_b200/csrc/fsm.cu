@@ -76,17 +76,7 @@ __device__ __forceinline__ bool contains(const uint32_t *list, uint32_t len, uin
 // CSR entries, claimed in chunks from a counter, so a hub's pairs spread over many warps instead of
 // one warp walking d(v0)^2 d(v1) / 32 steps alone.
 
-// The positions before the last one are the same for every embedding a warp step finds, so they
-// are marked once per distinct candidate of the step (the first lane of each group of lanes that
-// found the same candidate marks them); every lane marks its own last vertex.
-__device__ __forceinline__ void mark_prefix(const FsmArgs &a, int c, int k, const uint32_t *v) {
-    const unsigned peers = __match_any_sync(__activemask(), c);
-    if ((int)lane_id() == __ffs(peers) - 1)
-        for (int p = 0; p + 1 < k; ++p) mark(a, c, p, v[p]);
-    mark(a, c, k - 1, v[k - 1]);
-}
-
-// the embeddings that extend the pair (v0, v1); lanes take the last vertex
+// the embeddings that extend the pair (v0, v1 = N(v0)[i1]); lanes take the last vertex
 template <int T>
 __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t v1) {
     const unsigned lane = lane_id();
@@ -102,15 +92,12 @@ __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t
     if constexpr (T == kWedge || T == kTriangle) {
         for (uint32_t i = lane; i < d0; i += 32) {
             const uint32_t v2 = __ldg(n0 + i);
-            int c = -1;
-            if (v2 != v1) {
-                c = a.table[base01 + __ldg(a.labels + v2)];
-                if (T == kTriangle && c >= 0 && !contains(n1, d1, v2)) c = -1;
-            }
-            if (c >= 0) {
-                const uint32_t v[3] = {v0, v1, v2};
-                mark_prefix(a, c, 3, v);
-            }
+            if (v2 == v1) continue;
+            const int c = a.table[base01 + __ldg(a.labels + v2)];
+            if (c < 0) continue;
+            if (T == kTriangle && !contains(n1, d1, v2)) continue;
+            const uint32_t v[3] = {v0, v1, v2};
+            mark_all(a, c, 3, v);
         }
     } else {
         // four-chain: v2 from N(v0); three-star: v2 from N(v1)
@@ -124,11 +111,11 @@ __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t
             const uint32_t base012 = (base01 + l2) * L;
             for (uint32_t i = lane; i < d1; i += 32) {
                 const uint32_t v3 = __ldg(n1 + i);
-                const int c = (v3 == v0 || v3 == v2) ? -1 : a.table[base012 + __ldg(a.labels + v3)];
-                if (c >= 0) {
-                    const uint32_t v[4] = {v0, v1, v2, v3};
-                    mark_prefix(a, c, 4, v);
-                }
+                if (v3 == v0 || v3 == v2) continue;
+                const int c = a.table[base012 + __ldg(a.labels + v3)];
+                if (c < 0) continue;
+                const uint32_t v[4] = {v0, v1, v2, v3};
+                mark_all(a, c, 4, v);
             }
         }
     }
