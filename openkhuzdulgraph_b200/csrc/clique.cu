@@ -524,36 +524,51 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return done != 0;
 }
 
+// mbarriers of the tensor-core count: operand stage s full (producer warps arrived) and empty (its
+// MMAs completed), and the accumulators of a pass complete
+enum : int { kBarFull = 0, kBarEmpty = 2, kBarAcc = 4, kMmaBars = 5 };
+
 struct MmaState {
-    uint32_t tmem;       // tensor-memory base of the accumulators (G x 128 columns)
-    uint32_t mbar[2];    // shared addresses of the two stages' MMA-completion mbarriers
-    uint32_t phase[2];   // parity of each barrier's next completion
-    uint32_t pending[2]; // 1 while a commit to the barrier has not been waited for
-    int G;               // accumulator tiles per pass
-    uint8_t *stage;      // two stages of (G + 1) operand tiles each
+    uint32_t tmem;            // tensor-memory base of the accumulators (G x 128 columns)
+    uint32_t bar[kMmaBars];   // shared addresses of the mbarriers
+    uint32_t uses[2];         // fills of each operand stage so far (every thread keeps the count)
+    uint32_t passes;          // accumulator passes so far
+    int G;                    // accumulator tiles per pass
+    uint8_t *stage;           // two stages of (G + 1) operand tiles each
+    volatile int *abort;      // set when a wait ran out: every role then stops waiting
 };
 
-// wait for the MMAs last committed to stage st's barrier (block-uniform); false, with the stall
-// recorded and the commit left pending, after the poll limit
-__device__ __forceinline__ bool mma_stage_wait(MmaState &ms, int st, unsigned int *err) {
-    const bool ok = mbar_wait(ms.mbar[st], ms.phase[st]);
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) atomicOr(err, 2u);
-        return false;
+// poll an mbarrier phase; false after the poll limit, or early once another thread set the abort flag
+__device__ __forceinline__ bool mbar_wait_abortable(uint32_t mbar, uint32_t parity, volatile int *abort) {
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kMmaWaitIters && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (!done && (it & 63u) == 63u && *abort) break;
     }
-    ms.phase[st] ^= 1u;
-    ms.pending[st] = 0;
-    return true;
+    return done != 0;
 }
 
-// 4-clique count of one start vertex on the tensor cores.  The 32-column steps of a pass alternate
-// between two operand stages: step s expands into stage s & 1 while the MMAs of step s - 1 run, and
-// waits only for step s - 2 (the last reader of that stage).  Returns false (after recording the
-// stall in *err) if an MMA completion was not seen within the poll limit; the caller then stops.
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(mbar) : "memory");
+}
+
+// 4-clique count of one start vertex on the tensor cores, warp-specialised: warps 1.. expand the
+// operand tiles of each 32-column step into one of two stages and arrive on its `full` barrier;
+// thread 0 waits for it, issues the step's MMAs and commits them to the stage's `empty` barrier
+// (and, after a pass's last step, to the accumulator barrier).  Producers wait for `empty` only
+// before refilling a stage, so the expansion of step s + 1 overlaps the MMAs of step s, and no
+// block-wide barrier is taken per step; all warps then read the pass's accumulators.  Every wait is
+// bounded; one that runs out sets the abort flag, the others then give up at once, and the
+// function returns false with the stall recorded in *err.
 template <int THREADS>
 __device__ bool count_rows_mma(const Local &g, MmaState &ms, unsigned int *err, Acc &a) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int kWarps = THREADS / 32;
+    constexpr int kProducerThreads = THREADS - 32;
     const int d = g.d;
     // triangles through v0 (NumExtensions): every set bit of every row
     for (int i = tid; i < d; i += THREADS) {
@@ -570,41 +585,65 @@ __device__ bool count_rows_mma(const Local &g, MmaState &ms, unsigned int *err, 
             const int ng = min(ms.G, nb - jb0);
             const int k0 = jb0 * (kMmaRows / 32);
             for (int kc = k0; kc < kw; ++kc) {
-                const int st = (kc - k0) & 1;
-                if (ms.pending[st] && !mma_stage_wait(ms, st, err)) return false;
-                // stage st: tile 0 = rows of block ib, tile 1 + t = rows of block jb0 + t
+                const int st = (int)((ms.uses[0] + ms.uses[1]) & 1u);
+                const uint32_t u = ms.uses[st];
                 uint8_t *stage = ms.stage + st * stage_bytes;
-                for (int task = tid; task < (ng + 1) * kMmaRows; task += THREADS) {
-                    const int tile = task / kMmaRows, r = task % kMmaRows;
-                    const int R = (tile == 0 ? ib : jb0 + tile - 1) * kMmaRows + r;
-                    const uint32_t bits = R < d ? g.rows[(size_t)R * g.S + kc] : 0u;
-                    expand_row_bits(stage + tile * kMmaTileBytes, r, bits);
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncthreads();
-                if (tid == 0) {
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t s0 = smem_addr(stage);
-                    const uint64_t da = mma_desc(s0);
-                    const uint32_t acc = kc > k0 ? 1u : 0u;
-                    for (int t = 0; t < ng; ++t) {
-                        const uint64_t db = mma_desc(s0 + (uint32_t)(t + 1) * kMmaTileBytes);
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(
-                                ms.tmem + (uint32_t)(t * kMmaRows)),
-                            "l"(da), "l"(db), "r"(kMmaIdesc), "r"(acc), "r"(0u));
+                if (warp > 0) {
+                    // producers: refill the stage once its previous MMAs completed
+                    int go = 1;
+                    if (lane == 0) {
+                        if (u > 0 && !mbar_wait_abortable(ms.bar[kBarEmpty + st], (u - 1) & 1u, ms.abort)) *ms.abort = 1;
+                        go = !*ms.abort;
                     }
-                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                     ms.mbar[st])
-                                 : "memory");
+                    go = __shfl_sync(kFull, go, 0);
+                    if (go) {
+                        // tile 0 = rows of block ib, tile 1 + t = rows of block jb0 + t
+                        for (int task = tid - 32; task < (ng + 1) * kMmaRows; task += kProducerThreads) {
+                            const int tile = task / kMmaRows, r = task % kMmaRows;
+                            const int R = (tile == 0 ? ib : jb0 + tile - 1) * kMmaRows + r;
+                            const uint32_t bits = R < d ? g.rows[(size_t)R * g.S + kc] : 0u;
+                            expand_row_bits(stage + tile * kMmaTileBytes, r, bits);
+                        }
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(ms.bar[kBarFull + st]);
+                } else if (lane == 0) {
+                    // the MMA thread
+                    if (!mbar_wait_abortable(ms.bar[kBarFull + st], u & 1u, ms.abort)) *ms.abort = 1;
+                    if (!*ms.abort) {
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const uint32_t s0 = smem_addr(stage);
+                        const uint64_t da = mma_desc(s0);
+                        const uint32_t acc = kc > k0 ? 1u : 0u;
+                        for (int t = 0; t < ng; ++t) {
+                            const uint64_t db = mma_desc(s0 + (uint32_t)(t + 1) * kMmaTileBytes);
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(
+                                    ms.tmem + (uint32_t)(t * kMmaRows)),
+                                "l"(da), "l"(db), "r"(kMmaIdesc), "r"(acc), "r"(0u));
+                        }
+                        asm volatile(
+                            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                ms.bar[kBarEmpty + st])
+                            : "memory");
+                        if (kc == kw - 1)
+                            asm volatile(
+                                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                    ms.bar[kBarAcc])
+                                : "memory");
+                    }
                 }
-                ms.pending[st] = 1;
+                ms.uses[st] = u + 1;
             }
-            // the pass's last one or two steps are still outstanding, one per stage
-            for (int st = 0; st < 2; ++st)
-                if (ms.pending[st] && !mma_stage_wait(ms, st, err)) return false;
+            // the pass's accumulators
+            const bool ok = mbar_wait_abortable(ms.bar[kBarAcc], ms.passes & 1u, ms.abort);
+            ms.passes += 1;
+            if (__syncthreads_or(!ok || *ms.abort)) {
+                if (tid == 0) atomicOr(err, 2u);
+                return false;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows of block ib), columns
             // 16 c, 16 (c + kWarps / 4), ... of the ng accumulator tiles
@@ -789,8 +828,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
     extern __shared__ __align__(16) uint32_t smem[];
     __shared__ uint32_t s_v0;
     __shared__ int s_job;
-    __shared__ __align__(8) uint64_t s_mbar[2];
+    __shared__ __align__(8) uint64_t s_mbar[kMmaBars];
     __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
     const int dp = (dcap + 31) & ~31;
     const int logt = block_logt(dcap);
     const int T = 1 << logt;
@@ -806,8 +846,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
     uint32_t *ring = g.rows + block_rows_words(dcap) + (size_t)wib * kRing;
     const bool use_mma = kMma && mma_g > 0;
     const uint32_t tmem_cols = mma_tmem_cols(mma_g);
-    MmaState ms{0, {0, 0}, {0, 0}, {0, 0}, mma_g,
-                reinterpret_cast<uint8_t *>(g.rows + block_rows_words(dcap))};  // stages: over the rings
+    MmaState ms{0, {0, 0, 0, 0, 0}, {0, 0}, 0, mma_g,
+                reinterpret_cast<uint8_t *>(g.rows + block_rows_words(dcap)),  // stages: over the rings
+                &s_abort};
     if (use_mma) {
         if (wib == 0) {
             asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
@@ -815,16 +856,20 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
             asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
         }
         if (threadIdx.x == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar[0])));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar[1])));
+            // `full` waits for one arrival per producer warp (all warps but warp 0); the others for
+            // one tcgen05.commit
+            for (int b = 0; b < kMmaBars; ++b) {
+                const uint32_t count = b < kBarEmpty ? (uint32_t)(warps - 1) : 1u;
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s_mbar[b])), "r"(count));
+            }
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            s_abort = 0;
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         ms.tmem = s_tmem;
-        ms.mbar[0] = smem_addr(&s_mbar[0]);
-        ms.mbar[1] = smem_addr(&s_mbar[1]);
+        for (int b = 0; b < kMmaBars; ++b) ms.bar[b] = smem_addr(&s_mbar[b]);
     }
     bool stalled = false;
     const unsigned int n_list = *list_len;
@@ -885,9 +930,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == kLargeThreads ? 1 : (THREA
     if (use_mma) {
         // after a stall, give the outstanding MMAs one more bounded wait before the accumulators
         // are released (a completed phase makes the wait return at once)
-        if (stalled)
+        if (stalled && threadIdx.x == 0)
             for (int st = 0; st < 2; ++st)
-                if (ms.pending[st]) mbar_wait(ms.mbar[st], ms.phase[st]);
+                if (ms.uses[st] > 0) mbar_wait(ms.bar[kBarEmpty + st], (ms.uses[st] - 1) & 1u);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         if (wib == 0) {
