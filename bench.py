@@ -875,7 +875,7 @@ def main():
                     help="clique4: the bench line; batch: the uneven multi-graph batch; serve: Poisson serving; "
                          "configs: every app of the full-size configurations; app: one app (--app, --engine); "
                          "fsm: 3-FSM on labelled R-MAT graphs (--fsm-scales)")
-    ap.add_argument("--fsm-scales", type=int, nargs="+", default=[13, 14])
+    ap.add_argument("--fsm-scales", type=int, nargs="+", default=[13, 16, 18])
     ap.add_argument("--app", default="kautomine_four_motif", help="app of the app workload")
     ap.add_argument("--engine", default="auto", choices=["auto", "dfs", "bitmap", "wedge"],
                     help="engine of the app workload")

@@ -10,13 +10,15 @@
 // support is the least of these (get_support, engine.h:384-401).
 //
 // Where the reference runs the engine once per candidate (run(..., restrict_starting_vertex_label,
-// labels[0])), the device enumerates every embedding of a level's template once for all of the
-// level's candidates: each warp owns one start vertex v0, lanes take the last vertex's candidates
-// in parallel, and an embedding whose label tuple is a candidate (one lookup in a dense table
-// indexed by the labels) sets its vertices' bits in that candidate's per-position domain bitmaps
-// (a word is read before the atomicOr, so repeated images cost no atomics).  A popcount kernel then
-// gives every (candidate, position) domain size.  Candidates whose bitmaps would not fit the memory
-// budget at once are processed in groups.
+// labels[0])), the device answers all of a level's candidates at once.  Edges, wedges and triangles:
+// every embedding of the level's template is enumerated once (a warp per (v0, v1) pair, lanes over
+// the last vertex), and an embedding whose label tuple is a candidate (one lookup in a dense table
+// indexed by the labels) sets its vertices' bits in that candidate's per-position domain bitmaps (a
+// word is read before the atomicOr, so repeated images cost no atomics).  Four-chains and
+// three-stars, whose embeddings are far more numerous: each (candidate, position, vertex) is decided
+// by a search for one witness embedding over label counts of the neighbour lists (see below).  A
+// popcount kernel then gives every (candidate, position) domain size.  Candidates whose bitmaps
+// would not fit the memory budget at once are processed in groups.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,11 +74,12 @@ __device__ __forceinline__ bool contains(const uint32_t *list, uint32_t len, uin
 //   triangle    v1 in N(v0); v2 in N(v0) n N(v1)
 //   four-chain  v1 in N(v0); v2 in N(v0), v2 != v1; v3 in N(v1), v3 != v0, v3 != v2
 //   three-star  v1 in N(v0); v2 in N(v1), v2 != v0; v3 in N(v1), v3 != v0, v3 != v2
-// The edge template takes one warp per v0.  The others take one warp per (v0, v1) pair: pairs are
-// CSR entries, claimed in chunks from a counter, so a hub's pairs spread over many warps instead of
-// one warp walking d(v0)^2 d(v1) / 32 steps alone.
+// Edges, wedges and triangles are enumerated here (four-chains and three-stars by fsm_exist_kernel,
+// under the same constraints).  The edge template takes one warp per v0; wedges and triangles one
+// warp per (v0, v1) pair: pairs are CSR entries, claimed in chunks from a counter, so a hub's pairs
+// spread over many warps.
 
-// the embeddings that extend the pair (v0, v1 = N(v0)[i1]); lanes take the last vertex
+// the wedges or triangles that extend the pair (v0, v1); lanes take the last vertex
 template <int T>
 __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t v1) {
     const unsigned lane = lane_id();
@@ -89,35 +92,15 @@ __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t
     const uint32_t base01 = (l0 * L + l1) * L;
     const uint32_t *n1 = a.adj + a.off[v1];
     const uint32_t d1 = (uint32_t)(a.off[v1 + 1] - a.off[v1]);
-    if constexpr (T == kWedge || T == kTriangle) {
-        for (uint32_t i = lane; i < d0; i += 32) {
-            const uint32_t v2 = __ldg(n0 + i);
-            if (v2 == v1) continue;
-            const int c = a.table[base01 + __ldg(a.labels + v2)];
-            if (c < 0) continue;
-            if (T == kTriangle && !contains(n1, d1, v2)) continue;
-            const uint32_t v[3] = {v0, v1, v2};
-            mark_all(a, c, 3, v);
-        }
-    } else {
-        // four-chain: v2 from N(v0); three-star: v2 from N(v1)
-        const uint32_t *n2s = T == kFourChain ? n0 : n1;
-        const uint32_t d2s = T == kFourChain ? d0 : d1;
-        for (uint32_t i2 = 0; i2 < d2s; ++i2) {
-            const uint32_t v2 = __ldg(n2s + i2);
-            if (T == kFourChain ? v2 == v1 : v2 == v0) continue;
-            const uint32_t l2 = __ldg(a.labels + v2);
-            if (!a.pre2[base01 + l2]) continue;
-            const uint32_t base012 = (base01 + l2) * L;
-            for (uint32_t i = lane; i < d1; i += 32) {
-                const uint32_t v3 = __ldg(n1 + i);
-                if (v3 == v0 || v3 == v2) continue;
-                const int c = a.table[base012 + __ldg(a.labels + v3)];
-                if (c < 0) continue;
-                const uint32_t v[4] = {v0, v1, v2, v3};
-                mark_all(a, c, 4, v);
-            }
-        }
+    static_assert(T == kWedge || T == kTriangle, "four-chains and three-stars use fsm_exist_kernel");
+    for (uint32_t i = lane; i < d0; i += 32) {
+        const uint32_t v2 = __ldg(n0 + i);
+        if (v2 == v1) continue;
+        const int c = a.table[base01 + __ldg(a.labels + v2)];
+        if (c < 0) continue;
+        if (T == kTriangle && !contains(n1, d1, v2)) continue;
+        const uint32_t v[3] = {v0, v1, v2};
+        mark_all(a, c, 3, v);
     }
 }
 
@@ -159,6 +142,178 @@ __global__ void __launch_bounds__(256) fsm_domain_kernel(FsmArgs a) {
                 while (a.off[v0 + 1] <= e) ++v0;
                 fsm_pair<T>(a, v0, __ldg(a.adj + e));
             }
+        }
+    }
+}
+
+// ---- four-chain and three-star domains by existence -------------------------------------------
+// Enumerating every four-chain or three-star costs sum d(v0)^2 d(v1) steps (22 s at R-MAT scale 16),
+// while a domain only asks, per (candidate, position, vertex x), whether SOME embedding of the
+// enumeration above puts x at that position.  With lc(v, l), the number of neighbours of v with
+// label l, each such question needs one pass over a neighbour list (or two nested for the chain's
+// outer positions) and stops at the first witness.  The answers are the same sets the enumeration
+// marks, since the conditions below are exactly its constraints with the other vertices left free:
+//   four-chain v2 - v0 - v1 - v3 with labels (c0, c1, c2, c3), all four distinct;
+//   three-star: centre v1 (c1), leaves v0, v2, v3 (c0, c2, c3), all four distinct.
+
+// lc: one warp per vertex, a label histogram per warp in shared memory
+__global__ void __launch_bounds__(256) fsm_label_count_kernel(const uint64_t *__restrict__ off,
+                                                             const uint32_t *__restrict__ adj,
+                                                             const uint32_t *__restrict__ labels, uint32_t n,
+                                                             uint32_t L, uint32_t *lc) {
+    __shared__ uint32_t hist[8][kFsmMaxLabels];
+    const unsigned lane = lane_id();
+    const int wib = threadIdx.x >> 5;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = warp; v < n; v += nwarps) {
+        for (uint32_t l = lane; l < L; l += 32) hist[wib][l] = 0;
+        __syncwarp();
+        for (uint64_t e = off[v] + lane; e < off[v + 1]; e += 32) atomicAdd(&hist[wib][__ldg(labels + __ldg(adj + e))], 1u);
+        __syncwarp();
+        for (uint32_t l = lane; l < L; l += 32) lc[(size_t)v * L + l] = hist[wib][l];
+        __syncwarp();
+    }
+}
+
+struct FsmExistArgs {
+    const uint64_t *off;
+    const uint32_t *adj;
+    const uint32_t *labels;
+    const uint32_t *lc;      // n x L
+    uint32_t n;
+    uint32_t L;
+    const uint8_t *cands;    // per candidate of the group: its 4 labels in enumeration order
+    uint32_t num_cands;
+    uint32_t *domains;       // [candidate][position][words]
+    uint32_t words;
+    unsigned long long *queue;  // (candidate, vertex) claims, zeroed before the launch
+};
+
+__device__ __forceinline__ uint32_t lcount(const FsmExistArgs &a, uint32_t v, uint32_t l) {
+    return __ldg(a.lc + (size_t)v * a.L + l);
+}
+
+// four-chain: does the pair (v0, v1) (labels c0, c1, adjacent) extend by v2 in N(v0) with label c2
+// and v3 in N(v1) with label c3, all four distinct?  A and B count the choices left for v2 and v3;
+// only when each has exactly one and the labels agree must the two be compared (found by scans).
+__device__ bool chain_pair(const FsmExistArgs &a, uint32_t v0, uint32_t v1, uint32_t c0, uint32_t c1, uint32_t c2,
+                           uint32_t c3) {
+    const uint32_t A = lcount(a, v0, c2) - (c1 == c2 ? 1u : 0u);
+    const uint32_t B = lcount(a, v1, c3) - (c0 == c3 ? 1u : 0u);
+    if (A == 0 || B == 0) return false;
+    if (A >= 2 || B >= 2 || c2 != c3) return true;
+    uint32_t as = 0xffffffffu, bs = 0xffffffffu;
+    for (uint64_t e = a.off[v0]; e < a.off[v0 + 1]; ++e) {
+        const uint32_t u = __ldg(a.adj + e);
+        if (u != v1 && __ldg(a.labels + u) == c2) {
+            as = u;
+            break;
+        }
+    }
+    for (uint64_t e = a.off[v1]; e < a.off[v1 + 1]; ++e) {
+        const uint32_t w = __ldg(a.adj + e);
+        if (w != v0 && __ldg(a.labels + w) == c3) {
+            bs = w;
+            break;
+        }
+    }
+    return as != bs;
+}
+
+__device__ __forceinline__ bool has_nbr(const FsmExistArgs &a, uint32_t v, uint32_t x) {
+    const uint64_t b = a.off[v];
+    const uint32_t d = (uint32_t)(a.off[v + 1] - b);
+    const uint32_t p = lower_bound_u32(a.adj + b, 0, d, x);
+    return p < d && __ldg(a.adj + b + p) == x;
+}
+
+// three-star: with the leaf labels still to place as a multiset (up to 3 labels), does y have
+// enough neighbours of each label once `ex` (a neighbour of y with label lex, or none) is left out?
+__device__ __forceinline__ bool star_fits(const FsmExistArgs &a, uint32_t y, const uint32_t *need, int k,
+                                          int lex) {
+    for (int i = 0; i < k; ++i) {
+        uint32_t mult = 0;
+        for (int j = 0; j < k; ++j) mult += need[j] == need[i] ? 1u : 0u;
+        const uint32_t have = lcount(a, y, need[i]) - ((int)need[i] == lex ? 1u : 0u);
+        if (have < mult) return false;
+    }
+    return true;
+}
+
+// One warp per (candidate, vertex x); for each position whose label is x's, the warp looks for a
+// witness embedding and lane 0 sets x's domain bit.
+template <int T>
+__global__ void __launch_bounds__(256) fsm_exist_kernel(FsmExistArgs a) {
+    const unsigned lane = lane_id();
+    const uint64_t tasks = (uint64_t)a.num_cands * a.n;
+    while (true) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(a.queue, 1ull);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= tasks) break;
+        const uint32_t c = (uint32_t)(t / a.n), x = (uint32_t)(t % a.n);
+        const uint8_t *cl = a.cands + (size_t)c * 4;
+        const uint32_t c0 = cl[0], c1 = cl[1], c2 = cl[2], c3 = cl[3];
+        const uint32_t lx = __ldg(a.labels + x);
+        const uint64_t bx = a.off[x], ex = a.off[x + 1];
+        for (int p = 0; p < 4; ++p) {
+            if (cl[p] != lx) continue;
+            bool found = false;
+            if (T == kThreeStar && p == 1) {
+                const uint32_t need[3] = {c0, c2, c3};
+                found = star_fits(a, x, need, 3, -1);
+            } else if (T == kThreeStar) {
+                // x is leaf p: a centre y in N(x) with label c1 that still has the other two leaves
+                const uint32_t need[2] = {p == 0 ? c2 : c0, p == 3 ? c2 : c3};
+                for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
+                    bool hit = false;
+                    const uint64_t e = e0 + lane;
+                    if (e < ex) {
+                        const uint32_t y = __ldg(a.adj + e);
+                        hit = __ldg(a.labels + y) == c1 && star_fits(a, y, need, 2, (int)lx);
+                    }
+                    found = __any_sync(kFull, hit);
+                }
+            } else if (p <= 1) {
+                // four-chain, x = v0 (p = 0) or v1 (p = 1): a partner in N(x) completing the pair
+                const uint32_t want = p == 0 ? c1 : c0;
+                for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
+                    bool hit = false;
+                    const uint64_t e = e0 + lane;
+                    if (e < ex) {
+                        const uint32_t y = __ldg(a.adj + e);
+                        if (__ldg(a.labels + y) == want)
+                            hit = p == 0 ? chain_pair(a, x, y, c0, c1, c2, c3) : chain_pair(a, y, x, c0, c1, c2, c3);
+                    }
+                    found = __any_sync(kFull, hit);
+                }
+            } else {
+                // four-chain, x = v2 (p = 2): v0 in N(x) (c0), v1 in N(v0) \ {x} (c1), and v1 keeps a
+                // neighbour of label c3 other than v0 and x; x = v3 (p = 3) is the mirror image
+                // (v1 in N(x) (c1), v0 in N(v1) \ {x} (c0), v0 keeps a c2 neighbour other than v1, x)
+                const uint32_t lmid = p == 2 ? c0 : c1, lfar = p == 2 ? c1 : c0, lend = p == 2 ? c3 : c2;
+                const uint32_t lmid_in_end = lmid == lend ? 1u : 0u;
+                for (uint64_t e1 = bx; e1 < ex && !found; ++e1) {
+                    const uint32_t m = __ldg(a.adj + e1);  // v0 (p = 2) or v1 (p = 3), warp-uniform
+                    if (__ldg(a.labels + m) != lmid) continue;
+                    const uint64_t bm = a.off[m], em = a.off[m + 1];
+                    for (uint64_t e0 = bm; e0 < em && !found; e0 += 32) {
+                        bool hit = false;
+                        const uint64_t e = e0 + lane;
+                        if (e < em) {
+                            const uint32_t f = __ldg(a.adj + e);  // v1 (p = 2) or v0 (p = 3)
+                            if (f != x && __ldg(a.labels + f) == lfar) {
+                                const uint32_t k = lcount(a, f, lend) - lmid_in_end;
+                                hit = k >= 2 || (k == 1 && (lx != lend || !has_nbr(a, f, x)));
+                            }
+                        }
+                        found = __any_sync(kFull, hit);
+                    }
+                }
+            }
+            if (found && lane == 0)
+                atomicOr(a.domains + ((size_t)c * 4 + p) * a.words + (x >> 5), 1u << (x & 31));
         }
     }
 }
@@ -293,7 +448,8 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     const size_t group_max = std::max<size_t>(1, budget / per_cand);
     int32_t *d_table = nullptr;
     uint8_t *d_pre = nullptr;
-    uint32_t *d_dom = nullptr, *d_sizes = nullptr;
+    uint32_t *d_dom = nullptr, *d_sizes = nullptr, *d_lc = nullptr;
+    uint8_t *d_cands = nullptr;
     unsigned long long *d_queue = nullptr;
     auto release = [&]() {
         cudaFree(d_table);
@@ -301,12 +457,16 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
         cudaFree(d_dom);
         cudaFree(d_sizes);
         cudaFree(d_queue);
+        cudaFree(d_lc);
+        cudaFree(d_cands);
     };
     cudaError_t e = cudaMalloc(&d_table, sizeof(int32_t) * tsize);
     if (e == cudaSuccess) e = cudaMalloc(&d_pre, (size_t)L * L + (size_t)L * L * L);
     if (e == cudaSuccess) e = cudaMalloc(&d_dom, per_cand * group_max);
     if (e == cudaSuccess) e = cudaMalloc(&d_sizes, sizeof(uint32_t) * 4 * group_max);
     if (e == cudaSuccess) e = cudaMalloc(&d_queue, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&d_lc, sizeof(uint32_t) * std::max<size_t>((size_t)n * L, 1));
+    if (e == cudaSuccess) e = cudaMalloc(&d_cands, 4 * group_max);
     if (e != cudaSuccess) {
         cudaGetLastError();
         release();
@@ -317,8 +477,11 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)n + 7) / 8, (uint64_t)sms * 16));
+    // the label histogram of every neighbour list (the four-chain and three-star levels)
+    if (n > 0) fsm_label_count_kernel<<<grid, 256>>>(gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_lc);
     std::vector<int32_t> table(tsize);
     std::vector<uint8_t> pre((size_t)L * L + (size_t)L * L * L);
+    std::vector<uint8_t> cand_labels(4 * group_max);
     for (int t = kEdge; t <= kThreeStar; ++t) {
         const std::vector<Candidate> cands = candidates_of(t, L, f);
         const int k = kPatSize[t];
@@ -356,12 +519,22 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
             }
             FsmArgs a{gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_table, d_pre, d_pre + (size_t)L * L, d_dom, words,
                       gi.num_entries, d_queue};
+            if (k == 4) {
+                for (size_t c = 0; c < gn; ++c)
+                    for (int p = 0; p < 4; ++p) cand_labels[4 * c + p] = (uint8_t)cands[g0 + c].canonical[p];
+                if (cudaMemcpy(d_cands, cand_labels.data(), 4 * gn, cudaMemcpyHostToDevice) != cudaSuccess) {
+                    release();
+                    return cuda_fail(cudaGetLastError(), "3-FSM candidates");
+                }
+            }
+            FsmExistArgs x{gi.d_offsets, gi.d_adj, gi.d_labels, d_lc, n, L, d_cands, (uint32_t)gn, d_dom, words, d_queue};
+            const int xgrid = sms * 8;
             switch (t) {
                 case kEdge: fsm_domain_kernel<kEdge><<<grid, 256>>>(a); break;
                 case kWedge: fsm_domain_kernel<kWedge><<<grid, 256>>>(a); break;
                 case kTriangle: fsm_domain_kernel<kTriangle><<<grid, 256>>>(a); break;
-                case kFourChain: fsm_domain_kernel<kFourChain><<<grid, 256>>>(a); break;
-                default: fsm_domain_kernel<kThreeStar><<<grid, 256>>>(a); break;
+                case kFourChain: fsm_exist_kernel<kFourChain><<<xgrid, 256>>>(x); break;
+                default: fsm_exist_kernel<kThreeStar><<<xgrid, 256>>>(x); break;
             }
             fsm_popcount_kernel<<<(unsigned)(gn * k), 256>>>(d_dom, words, k, d_sizes);
             std::vector<uint32_t> sizes(gn * k);

@@ -28,6 +28,9 @@ GRAPHS = [
      "thresholds": [60]},
     {"name": "er_n3000_m20000_s5_l3", "kind": "er", "n": 3000, "m": 20000, "seed": 5, "labels": 3, "mult": 31,
      "thresholds": [300]},
+    # two labels: patterns with equal labels on symmetric positions, hubs of degree ~300
+    {"name": "rmat_s11_ef8_s4_l2", "kind": "rmat", "scale": 11, "ef": 8, "seed": 4, "labels": 2, "mult": 3,
+     "thresholds": [100, 400]},
 ]
 
 LEVELS = ["single-vertex", "single-edge", "wedge", "triangle", "four-chain", "three-star"]
