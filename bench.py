@@ -40,7 +40,9 @@ APP = "kautomine_four_clique"
 KNOWN_COUNTS = {(22, 16): 123601255038, (21, 16): 46044614288}
 SAMPLE_MOD = 32      # CPU sample: start vertices with v0 % 32 == 0 (one label class of 32)
 METRIC = "embeddings/s (4-clique, exact uint64 count)"
-WORKLOAD = "4-clique count, R-MAT scale 22 ef 16 (a,b,c)=(0.57,0.19,0.19) seed 1, degree-oriented DAG"
+def workload_name(scale=SCALE, edge_factor=EDGE_FACTOR):
+    return ("4-clique count, R-MAT scale %d ef %d (a,b,c)=(0.57,0.19,0.19) seed 1, degree-oriented DAG"
+            % (scale, edge_factor))
 
 
 def peaks():
@@ -391,7 +393,7 @@ def ours(args, rank, world, local):
             "metric": METRIC, "value": value, "unit": "embeddings/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic (device R-MAT generator)",
-            "config": {"workload": WORKLOAD, "vertices": n, "oriented_edges": m,
+            "config": {"workload": workload_name(args.scale, args.edge_factor), "vertices": n, "oriented_edges": m,
                        "undirected_edges": sym_info.num_entries // 2, "max_out_degree": gi.max_degree,
                        "count": ref_counts[0], "num_extensions": st_stats.num_extensions,
                        "embeddings_per_step": embeddings, "parallelism": "replicas" if world > 1 else "single",
@@ -850,7 +852,8 @@ def reference_arm(args, rank, world, local):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "embeddings/s", "n_gpus": 0,
             "steps": args.steps, "warmup": 0, "ms_per_step": r["secs"] * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": "v0 %% %d == 0" % SAMPLE_MOD, "same_config": False,
+            "config": {"workload": workload_name(args.scale, args.edge_factor), "sample": "v0 %% %d == 0" % SAMPLE_MOD,
+                       "same_config": False,
                        "graph_built_by": "oracle generator + reference converter + to_oriented_dataset_converter",
                        "graph_build_s": t_build},
             "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": cores, "threads": r["threads"],
