@@ -241,79 +241,133 @@ __device__ __forceinline__ bool star_fits(const FsmExistArgs &a, uint32_t y, con
     return true;
 }
 
-// One warp per (candidate, vertex x); for each position whose label is x's, the warp looks for a
-// witness embedding and lane 0 sets x's domain bit.
+__device__ __forceinline__ void set_domain_bit(const FsmExistArgs &a, uint32_t c, int p, uint32_t x) {
+    atomicOr(a.domains + ((size_t)c * 4 + p) * a.words + (x >> 5), 1u << (x & 31));
+}
+
+// The positions p of candidate c (labels c0..c3) that x, with label lx, could take: cl[p] == lx and
+// x's own label counts allow the position (necessary conditions of the searches below, so a
+// position dropped here has no witness).  The three-star centre needs only x's label counts and is
+// decided here outright.
+template <int T>
+__device__ __forceinline__ unsigned open_positions(const FsmExistArgs &a, uint32_t c, uint32_t x, uint32_t lx,
+                                                   uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
+    unsigned pm = 0;
+    if (T == kFourChain) {
+        // v0: a c1 neighbour and another c2 one; v1: a c0 neighbour and another c3 one;
+        // v2: a c0 neighbour; v3: a c1 neighbour
+        if (c0 == lx && lcount(a, x, c1) >= 1 && lcount(a, x, c2) >= 1 + (c1 == c2 ? 1u : 0u)) pm |= 1;
+        if (c1 == lx && lcount(a, x, c0) >= 1 && lcount(a, x, c3) >= 1 + (c0 == c3 ? 1u : 0u)) pm |= 2;
+        if (c2 == lx && lcount(a, x, c0) >= 1) pm |= 4;
+        if (c3 == lx && lcount(a, x, c1) >= 1) pm |= 8;
+    } else {
+        if (c1 == lx) {
+            const uint32_t need[3] = {c0, c2, c3};
+            if (star_fits(a, x, need, 3, -1)) set_domain_bit(a, c, 1, x);
+        }
+        // a leaf needs a neighbour with the centre's label
+        if ((c0 == lx || c2 == lx || c3 == lx) && lcount(a, x, c1) >= 1) {
+            if (c0 == lx) pm |= 1;
+            if (c2 == lx) pm |= 4;
+            if (c3 == lx) pm |= 8;
+        }
+    }
+    return pm;
+}
+
+// A warp claims 32 consecutive (candidate, vertex x) tasks at a time; each lane screens one of them
+// (open_positions), and the warp then searches a witness embedding for every position left open,
+// lane 0 setting x's domain bit when one is found.
 template <int T>
 __global__ void __launch_bounds__(256) fsm_exist_kernel(FsmExistArgs a) {
     const unsigned lane = lane_id();
     const uint64_t tasks = (uint64_t)a.num_cands * a.n;
     while (true) {
-        unsigned long long t = 0;
-        if (lane == 0) t = atomicAdd(a.queue, 1ull);
-        t = __shfl_sync(kFull, t, 0);
-        if (t >= tasks) break;
-        const uint32_t c = (uint32_t)(t / a.n), x = (uint32_t)(t % a.n);
-        const uint8_t *cl = a.cands + (size_t)c * 4;
-        const uint32_t c0 = cl[0], c1 = cl[1], c2 = cl[2], c3 = cl[3];
-        const uint32_t lx = __ldg(a.labels + x);
-        const uint64_t bx = a.off[x], ex = a.off[x + 1];
-        for (int p = 0; p < 4; ++p) {
-            if (cl[p] != lx) continue;
-            bool found = false;
-            if (T == kThreeStar && p == 1) {
-                const uint32_t need[3] = {c0, c2, c3};
-                found = star_fits(a, x, need, 3, -1);
-            } else if (T == kThreeStar) {
-                // x is leaf p: a centre y in N(x) with label c1 that still has the other two leaves
-                const uint32_t need[2] = {p == 0 ? c2 : c0, p == 3 ? c2 : c3};
-                for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
-                    bool hit = false;
-                    const uint64_t e = e0 + lane;
-                    if (e < ex) {
-                        const uint32_t y = __ldg(a.adj + e);
-                        hit = __ldg(a.labels + y) == c1 && star_fits(a, y, need, 2, (int)lx);
-                    }
-                    found = __any_sync(kFull, hit);
-                }
-            } else if (p <= 1) {
-                // four-chain, x = v0 (p = 0) or v1 (p = 1): a partner in N(x) completing the pair
-                const uint32_t want = p == 0 ? c1 : c0;
-                for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
-                    bool hit = false;
-                    const uint64_t e = e0 + lane;
-                    if (e < ex) {
-                        const uint32_t y = __ldg(a.adj + e);
-                        if (__ldg(a.labels + y) == want)
-                            hit = p == 0 ? chain_pair(a, x, y, c0, c1, c2, c3) : chain_pair(a, y, x, c0, c1, c2, c3);
-                    }
-                    found = __any_sync(kFull, hit);
-                }
-            } else {
-                // four-chain, x = v2 (p = 2): v0 in N(x) (c0), v1 in N(v0) \ {x} (c1), and v1 keeps a
-                // neighbour of label c3 other than v0 and x; x = v3 (p = 3) is the mirror image
-                // (v1 in N(x) (c1), v0 in N(v1) \ {x} (c0), v0 keeps a c2 neighbour other than v1, x)
-                const uint32_t lmid = p == 2 ? c0 : c1, lfar = p == 2 ? c1 : c0, lend = p == 2 ? c3 : c2;
-                const uint32_t lmid_in_end = lmid == lend ? 1u : 0u;
-                for (uint64_t e1 = bx; e1 < ex && !found; ++e1) {
-                    const uint32_t m = __ldg(a.adj + e1);  // v0 (p = 2) or v1 (p = 3), warp-uniform
-                    if (__ldg(a.labels + m) != lmid) continue;
-                    const uint64_t bm = a.off[m], em = a.off[m + 1];
-                    for (uint64_t e0 = bm; e0 < em && !found; e0 += 32) {
+        unsigned long long t0 = 0;
+        if (lane == 0) t0 = atomicAdd(a.queue, 32ull);
+        t0 = __shfl_sync(kFull, t0, 0);
+        if (t0 >= tasks) break;
+        const uint64_t t = t0 + lane;
+        uint32_t tc = 0, tx = 0;
+        unsigned tpm = 0;
+        if (t < tasks) {
+            tc = (uint32_t)(t / a.n);
+            tx = (uint32_t)(t % a.n);
+            const uint8_t *cl = a.cands + (size_t)tc * 4;
+            tpm = open_positions<T>(a, tc, tx, __ldg(a.labels + tx), cl[0], cl[1], cl[2], cl[3]);
+        }
+        for (unsigned todo = __ballot_sync(kFull, tpm != 0); todo; todo &= todo - 1) {
+            const int src = __ffs(todo) - 1;
+            const uint32_t c = __shfl_sync(kFull, tc, src), x = __shfl_sync(kFull, tx, src);
+            const unsigned pm = __shfl_sync(kFull, tpm, src);
+            const uint8_t *cl = a.cands + (size_t)c * 4;
+            const uint32_t c0 = cl[0], c1 = cl[1], c2 = cl[2], c3 = cl[3];
+            const uint32_t lx = __ldg(a.labels + x);
+            const uint64_t bx = a.off[x], ex = a.off[x + 1];
+            for (int p = 0; p < 4; ++p) {
+                if (!(pm >> p & 1)) continue;
+                bool found = false;
+                if (T == kThreeStar) {
+                    // x is leaf p: a centre y in N(x) with label c1 that still has the other two leaves
+                    const uint32_t need[2] = {p == 0 ? c2 : c0, p == 3 ? c2 : c3};
+                    for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
                         bool hit = false;
                         const uint64_t e = e0 + lane;
-                        if (e < em) {
-                            const uint32_t f = __ldg(a.adj + e);  // v1 (p = 2) or v0 (p = 3)
-                            if (f != x && __ldg(a.labels + f) == lfar) {
-                                const uint32_t k = lcount(a, f, lend) - lmid_in_end;
-                                hit = k >= 2 || (k == 1 && (lx != lend || !has_nbr(a, f, x)));
-                            }
+                        if (e < ex) {
+                            const uint32_t y = __ldg(a.adj + e);
+                            hit = __ldg(a.labels + y) == c1 && star_fits(a, y, need, 2, (int)lx);
                         }
                         found = __any_sync(kFull, hit);
                     }
+                } else if (p <= 1) {
+                    // four-chain, x = v0 (p = 0) or v1 (p = 1): a partner in N(x) completing the pair
+                    const uint32_t want = p == 0 ? c1 : c0;
+                    for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
+                        bool hit = false;
+                        const uint64_t e = e0 + lane;
+                        if (e < ex) {
+                            const uint32_t y = __ldg(a.adj + e);
+                            if (__ldg(a.labels + y) == want)
+                                hit = p == 0 ? chain_pair(a, x, y, c0, c1, c2, c3) : chain_pair(a, y, x, c0, c1, c2, c3);
+                        }
+                        found = __any_sync(kFull, hit);
+                    }
+                } else {
+                    // four-chain, x = v2 (p = 2): v0 in N(x) (c0), v1 in N(v0) \ {x} (c1), and v1 keeps a
+                    // neighbour of label c3 other than v0 and x; x = v3 (p = 3) is the mirror image
+                    // (v1 in N(x) (c1), v0 in N(v1) \ {x} (c0), v0 keeps a c2 neighbour other than v1, x).
+                    // The middle vertices m are screened 32 at a time: label lmid and an lfar neighbour
+                    // other than x.
+                    const uint32_t lmid = p == 2 ? c0 : c1, lfar = p == 2 ? c1 : c0, lend = p == 2 ? c3 : c2;
+                    const uint32_t lmid_in_end = lmid == lend ? 1u : 0u;
+                    const uint32_t far_min = 1u + (lx == lfar ? 1u : 0u);
+                    for (uint64_t g0 = bx; g0 < ex && !found; g0 += 32) {
+                        uint32_t mm = 0;
+                        bool ok = false;
+                        if (g0 + lane < ex) {
+                            mm = __ldg(a.adj + g0 + lane);
+                            ok = __ldg(a.labels + mm) == lmid && lcount(a, mm, lfar) >= far_min;
+                        }
+                        for (unsigned mids = __ballot_sync(kFull, ok); mids && !found; mids &= mids - 1) {
+                            const uint32_t m = __shfl_sync(kFull, mm, __ffs(mids) - 1);  // v0 (p = 2) or v1 (p = 3)
+                            const uint64_t bm = a.off[m], em = a.off[m + 1];
+                            for (uint64_t e0 = bm; e0 < em && !found; e0 += 32) {
+                                bool hit = false;
+                                const uint64_t e = e0 + lane;
+                                if (e < em) {
+                                    const uint32_t f = __ldg(a.adj + e);  // v1 (p = 2) or v0 (p = 3)
+                                    if (f != x && __ldg(a.labels + f) == lfar) {
+                                        const uint32_t k = lcount(a, f, lend) - lmid_in_end;
+                                        hit = k >= 2 || (k == 1 && (lx != lend || !has_nbr(a, f, x)));
+                                    }
+                                }
+                                found = __any_sync(kFull, hit);
+                            }
+                        }
+                    }
                 }
+                if (found && lane == 0) set_domain_bit(a, c, p, x);
             }
-            if (found && lane == 0)
-                atomicOr(a.domains + ((size_t)c * 4 + p) * a.words + (x >> 5), 1u << (x & 31));
         }
     }
 }
@@ -445,7 +499,8 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     KHZ_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t budget = std::max<size_t>(free_b / 4, (size_t)64 << 20);
     const size_t per_cand = (size_t)4 * words * sizeof(uint32_t);
-    const size_t group_max = std::max<size_t>(1, budget / per_cand);
+    // no level has more than L^4 candidates, so a larger buffer would only cost allocation time
+    const size_t group_max = std::max<size_t>(1, std::min(budget / per_cand, tsize));
     int32_t *d_table = nullptr;
     uint8_t *d_pre = nullptr;
     uint32_t *d_dom = nullptr, *d_sizes = nullptr, *d_lc = nullptr;
