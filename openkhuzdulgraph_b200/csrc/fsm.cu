@@ -10,13 +10,14 @@
 // support is the least of these (get_support, engine.h:384-401).
 //
 // Where the reference runs the engine once per candidate (run(..., restrict_starting_vertex_label,
-// labels[0])), the device answers all of a level's candidates at once.  Edges, wedges and triangles:
-// every embedding of the level's template is enumerated once (a warp per (v0, v1) pair, lanes over
-// the last vertex), and an embedding whose label tuple is a candidate (one lookup in a dense table
-// indexed by the labels) sets its vertices' bits in that candidate's per-position domain bitmaps (a
-// word is read before the atomicOr, so repeated images cost no atomics).  Four-chains and
-// three-stars, whose embeddings are far more numerous: each (candidate, position, vertex) is decided
-// by a search for one witness embedding over label counts of the neighbour lists (see below).  A
+// labels[0])), the device answers all of a level's candidates at once.  Edges and triangles: every
+// embedding of the level's template is enumerated once (a warp per v0, or per (v0, v1) pair with
+// lanes over the last vertex), and an embedding whose label tuple is a candidate (one lookup in a
+// dense table indexed by the labels) sets its vertices' bits in that candidate's per-position domain
+// bitmaps (a word is read before the atomicOr, so repeated images cost no atomics).  Wedges,
+// four-chains and three-stars, whose embeddings are far more numerous: each (candidate, position,
+// vertex) is decided by a search for one witness embedding over label counts of the neighbour lists
+// (see below).  A
 // popcount kernel then gives every (candidate, position) domain size.  Candidates whose bitmaps
 // would not fit the memory budget at once are processed in groups.
 #include <cuda_runtime.h>
@@ -74,12 +75,12 @@ __device__ __forceinline__ bool contains(const uint32_t *list, uint32_t len, uin
 //   triangle    v1 in N(v0); v2 in N(v0) n N(v1)
 //   four-chain  v1 in N(v0); v2 in N(v0), v2 != v1; v3 in N(v1), v3 != v0, v3 != v2
 //   three-star  v1 in N(v0); v2 in N(v1), v2 != v0; v3 in N(v1), v3 != v0, v3 != v2
-// Edges, wedges and triangles are enumerated here (four-chains and three-stars by fsm_exist_kernel,
-// under the same constraints).  The edge template takes one warp per v0; wedges and triangles one
-// warp per (v0, v1) pair: pairs are CSR entries, claimed in chunks from a counter, so a hub's pairs
-// spread over many warps.
+// Edges and triangles are enumerated here (wedges, four-chains and three-stars by fsm_exist_kernel,
+// under the same constraints).  The edge template takes one warp per v0; triangles one warp per
+// (v0, v1) pair: pairs are CSR entries, claimed in chunks from a counter, so a hub's pairs spread
+// over many warps.
 
-// the wedges or triangles that extend the pair (v0, v1); lanes take the last vertex
+// the triangles that extend the pair (v0, v1); lanes take the last vertex
 template <int T>
 __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t v1) {
     const unsigned lane = lane_id();
@@ -92,13 +93,13 @@ __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t
     const uint32_t base01 = (l0 * L + l1) * L;
     const uint32_t *n1 = a.adj + a.off[v1];
     const uint32_t d1 = (uint32_t)(a.off[v1 + 1] - a.off[v1]);
-    static_assert(T == kWedge || T == kTriangle, "four-chains and three-stars use fsm_exist_kernel");
+    static_assert(T == kTriangle, "wedges, four-chains and three-stars use fsm_exist_kernel");
     for (uint32_t i = lane; i < d0; i += 32) {
         const uint32_t v2 = __ldg(n0 + i);
         if (v2 == v1) continue;
         const int c = a.table[base01 + __ldg(a.labels + v2)];
         if (c < 0) continue;
-        if (T == kTriangle && !contains(n1, d1, v2)) continue;
+        if (!contains(n1, d1, v2)) continue;
         const uint32_t v[3] = {v0, v1, v2};
         mark_all(a, c, 3, v);
     }
@@ -146,13 +147,15 @@ __global__ void __launch_bounds__(256) fsm_domain_kernel(FsmArgs a) {
     }
 }
 
-// ---- four-chain and three-star domains by existence -------------------------------------------
+// ---- wedge, four-chain and three-star domains by existence ------------------------------------
 // Enumerating every four-chain or three-star costs sum d(v0)^2 d(v1) steps (22 s at R-MAT scale 16),
-// while a domain only asks, per (candidate, position, vertex x), whether SOME embedding of the
-// enumeration above puts x at that position.  With lc(v, l), the number of neighbours of v with
-// label l, each such question needs one pass over a neighbour list (or two nested for the chain's
-// outer positions) and stops at the first witness.  The answers are the same sets the enumeration
-// marks, since the conditions below are exactly its constraints with the other vertices left free:
+// every wedge sum d(v0)^2, while a domain only asks, per (candidate, position, vertex x), whether
+// SOME embedding of the enumeration above puts x at that position.  With lc(v, l), the number of
+// neighbours of v with label l, each such question needs at most one pass over a neighbour list (or
+// two nested for the chain's outer positions) and stops at the first witness.  The answers are the
+// same sets the enumeration marks, since the conditions below are exactly its constraints with the
+// other vertices left free:
+//   wedge v1 - v0 - v2 with labels (c0, c1, c2), all three distinct;
 //   four-chain v2 - v0 - v1 - v3 with labels (c0, c1, c2, c3), all four distinct;
 //   three-star: centre v1 (c1), leaves v0, v2, v3 (c0, c2, c3), all four distinct.
 
@@ -253,7 +256,15 @@ template <int T>
 __device__ __forceinline__ unsigned open_positions(const FsmExistArgs &a, uint32_t c, uint32_t x, uint32_t lx,
                                                    uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
     unsigned pm = 0;
-    if (T == kFourChain) {
+    if (T == kWedge) {
+        // centre v0: a c1 neighbour and another c2 one, decided here; ends v1 / v2: a c0 neighbour
+        const uint32_t same = c1 == c2 ? 1u : 0u;
+        if (c0 == lx && lcount(a, x, c1) >= 1 && lcount(a, x, c2) >= 1 + same) set_domain_bit(a, c, 0, x);
+        if ((c1 == lx || c2 == lx) && lcount(a, x, c0) >= 1) {
+            if (c1 == lx) pm |= 2;
+            if (c2 == lx) pm |= 4;
+        }
+    } else if (T == kFourChain) {
         // v0: a c1 neighbour and another c2 one; v1: a c0 neighbour and another c3 one;
         // v2: a c0 neighbour; v3: a c1 neighbour
         if (c0 == lx && lcount(a, x, c1) >= 1 && lcount(a, x, c2) >= 1 + (c1 == c2 ? 1u : 0u)) pm |= 1;
@@ -307,7 +318,21 @@ __global__ void __launch_bounds__(256) fsm_exist_kernel(FsmExistArgs a) {
             for (int p = 0; p < 4; ++p) {
                 if (!(pm >> p & 1)) continue;
                 bool found = false;
-                if (T == kThreeStar) {
+                if (T == kWedge) {
+                    // x is end p: a centre y in N(x) with label c0 and a neighbour of the other end's
+                    // label other than x
+                    const uint32_t lend = p == 1 ? c2 : c1;
+                    const uint32_t end_min = 1u + (c1 == c2 ? 1u : 0u);
+                    for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
+                        bool hit = false;
+                        const uint64_t e = e0 + lane;
+                        if (e < ex) {
+                            const uint32_t y = __ldg(a.adj + e);
+                            hit = __ldg(a.labels + y) == c0 && lcount(a, y, lend) >= end_min;
+                        }
+                        found = __any_sync(kFull, hit);
+                    }
+                } else if (T == kThreeStar) {
                     // x is leaf p: a centre y in N(x) with label c1 that still has the other two leaves
                     const uint32_t need[2] = {p == 0 ? c2 : c0, p == 3 ? c2 : c3};
                     for (uint64_t e0 = bx; e0 < ex && !found; e0 += 32) {
@@ -574,9 +599,10 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
             }
             FsmArgs a{gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_table, d_pre, d_pre + (size_t)L * L, d_dom, words,
                       gi.num_entries, d_queue};
-            if (k == 4) {
+            if (t == kWedge || k == 4) {
                 for (size_t c = 0; c < gn; ++c)
-                    for (int p = 0; p < 4; ++p) cand_labels[4 * c + p] = (uint8_t)cands[g0 + c].canonical[p];
+                    for (int p = 0; p < 4; ++p)
+                        cand_labels[4 * c + p] = p < k ? (uint8_t)cands[g0 + c].canonical[p] : (uint8_t)0;
                 if (cudaMemcpy(d_cands, cand_labels.data(), 4 * gn, cudaMemcpyHostToDevice) != cudaSuccess) {
                     release();
                     return cuda_fail(cudaGetLastError(), "3-FSM candidates");
@@ -586,7 +612,7 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
             const int xgrid = sms * 8;
             switch (t) {
                 case kEdge: fsm_domain_kernel<kEdge><<<grid, 256>>>(a); break;
-                case kWedge: fsm_domain_kernel<kWedge><<<grid, 256>>>(a); break;
+                case kWedge: fsm_exist_kernel<kWedge><<<xgrid, 256>>>(x); break;
                 case kTriangle: fsm_domain_kernel<kTriangle><<<grid, 256>>>(a); break;
                 case kFourChain: fsm_exist_kernel<kFourChain><<<xgrid, 256>>>(x); break;
                 default: fsm_exist_kernel<kThreeStar><<<xgrid, 256>>>(x); break;
