@@ -195,7 +195,8 @@ int khz_app_multiplicity(khz_app_id app, int pattern);
  * pattern is frequent when its MNI support (for every pattern vertex the number of distinct graph
  * vertices it maps to, the least of these: SharedMemoryPatternDomain::get_support,
  * engine.h:384-401) reaches `threshold`.  The graph must carry node labels (at most 48, the
- * reference's MAX_NUM_LABELS).  out->level[i] gives what the app prints per level (the number of
+ * reference's MAX_NUM_LABELS) and be the symmetric CSR of a validated graph (the undirected form
+ * the app mines; KHZ_ERR_ARG otherwise, as for a graph without labels).  out->level[i] gives what the app prints per level (the number of
  * frequent patterns and the support sum; level 0's sum covers every label, as setup() computes
  * it).  patterns (may be NULL) receives up to `capacity` frequent canonical patterns in the order
  * found; *num_patterns their total number. */

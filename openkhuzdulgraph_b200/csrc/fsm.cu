@@ -78,30 +78,54 @@ __device__ __forceinline__ bool contains(const uint32_t *list, uint32_t len, uin
 // Edges and triangles are enumerated here (wedges, four-chains and three-stars by fsm_exist_kernel,
 // under the same constraints).  The edge template takes one warp per v0; triangles one warp per
 // (v0, v1) pair: pairs are CSR entries, claimed in chunks from a counter, so a hub's pairs spread
-// over many warps.
+// over many warps.  All of it assumes the symmetric CSR of a simple graph (validated: no self-loops),
+// which khz_fsm requires.
 
-// the triangles that extend the pair (v0, v1); lanes take the last vertex
+// (degree, id) order: each triangle is listed once, from its lowest-ranked vertex
+__device__ __forceinline__ bool ranks_below(uint32_t da, uint32_t va, uint32_t db, uint32_t vb) {
+    return da < db || (da == db && va < vb);
+}
+
+__device__ __forceinline__ void mark_tri(const FsmArgs &a, int cand, uint32_t x, uint32_t y, uint32_t z) {
+    if (cand < 0) return;
+    mark(a, cand, 0, x);
+    mark(a, cand, 1, y);
+    mark(a, cand, 2, z);
+}
+
+// the triangles {v0, v1, v2} with v0 < v1 < v2 in (degree, id) order; lanes take v2.  The app's
+// enumeration reaches each triangle of a symmetric graph in all six vertex orders, so every order
+// whose label tuple is a candidate is marked here.  Listing from the lowest-ranked vertex scans
+// sum d(v0) d+(v0) entries, d+ the neighbours ranked above v0, instead of sum d(v0)^2.
 template <int T>
 __device__ __forceinline__ void fsm_pair(const FsmArgs &a, uint32_t v0, uint32_t v1) {
+    static_assert(T == kTriangle, "wedges, four-chains and three-stars use fsm_exist_kernel");
     const unsigned lane = lane_id();
+    const uint64_t b0 = a.off[v0], b1 = a.off[v1];
+    const uint32_t d0 = (uint32_t)(a.off[v0 + 1] - b0);
+    const uint32_t d1 = (uint32_t)(a.off[v1 + 1] - b1);
+    if (!ranks_below(d0, v0, d1, v1)) return;
     const uint32_t L = a.L;
     const uint32_t l0 = __ldg(a.labels + v0);
     const uint32_t l1 = __ldg(a.labels + v1);
-    if (!a.pre1[l0 * L + l1]) return;
-    const uint32_t *n0 = a.adj + a.off[v0];
-    const uint32_t d0 = (uint32_t)(a.off[v0 + 1] - a.off[v0]);
-    const uint32_t base01 = (l0 * L + l1) * L;
-    const uint32_t *n1 = a.adj + a.off[v1];
-    const uint32_t d1 = (uint32_t)(a.off[v1 + 1] - a.off[v1]);
-    static_assert(T == kTriangle, "wedges, four-chains and three-stars use fsm_exist_kernel");
+    const uint32_t *n0 = a.adj + b0;
+    const uint32_t *n1 = a.adj + b1;
     for (uint32_t i = lane; i < d0; i += 32) {
         const uint32_t v2 = __ldg(n0 + i);
-        if (v2 == v1) continue;
-        const int c = a.table[base01 + __ldg(a.labels + v2)];
-        if (c < 0) continue;
+        const uint32_t d2 = (uint32_t)(a.off[v2 + 1] - a.off[v2]);
+        if (!ranks_below(d1, v1, d2, v2)) continue;
+        const uint32_t l2 = __ldg(a.labels + v2);
+        const int c012 = a.table[(l0 * L + l1) * L + l2], c021 = a.table[(l0 * L + l2) * L + l1];
+        const int c102 = a.table[(l1 * L + l0) * L + l2], c120 = a.table[(l1 * L + l2) * L + l0];
+        const int c201 = a.table[(l2 * L + l0) * L + l1], c210 = a.table[(l2 * L + l1) * L + l0];
+        if (c012 < 0 && c021 < 0 && c102 < 0 && c120 < 0 && c201 < 0 && c210 < 0) continue;
         if (!contains(n1, d1, v2)) continue;
-        const uint32_t v[3] = {v0, v1, v2};
-        mark_all(a, c, 3, v);
+        mark_tri(a, c012, v0, v1, v2);
+        mark_tri(a, c021, v0, v2, v1);
+        mark_tri(a, c102, v1, v0, v2);
+        mark_tri(a, c120, v1, v2, v0);
+        mark_tri(a, c201, v2, v0, v1);
+        mark_tri(a, c210, v2, v1, v0);
     }
 }
 
@@ -481,6 +505,10 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     if (st) return st;
     if (!gi.d_labels || gi.num_labels == 0) {
         set_error("3-FSM needs a graph with node labels");
+        return KHZ_ERR_ARG;
+    }
+    if (!gi.symmetric) {
+        set_error("3-FSM needs the symmetric (undirected) CSR of a validated graph");
         return KHZ_ERR_ARG;
     }
     if (gi.num_labels > (uint32_t)kFsmMaxLabels) {

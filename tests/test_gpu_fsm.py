@@ -5,6 +5,7 @@ import json
 import os
 import sys
 
+import numpy as np
 import pytest
 
 from conftest import ROOT
@@ -50,3 +51,18 @@ def test_fsm_needs_labels(khz_ctx):
         khz_ctx.fsm(g, 5)
     assert e.value.status == 1
     g.free()
+
+
+def test_fsm_needs_symmetric_graph(khz_ctx):
+    """The domains assume the undirected CSR: a graph stored one way round is refused."""
+    from openkhuzdulgraph_b200 import khz
+    import orc
+    canon, n = orc.er(60, 150, seed=2)
+    g = khz_ctx.graph_from_edges(canon, n)
+    try:
+        g.set_labels(np.arange(n, dtype=np.uint32) % 3)
+        with pytest.raises(khz.KhzError) as e:
+            khz_ctx.fsm(g, 5)
+        assert e.value.status == 1
+    finally:
+        g.free()
