@@ -45,8 +45,6 @@ struct FsmArgs {
     uint32_t n;
     uint32_t L;             // number of labels
     const int32_t *table;   // L^size entries: candidate index of a label tuple (group-local), or -1
-    const uint8_t *pre1;    // L^2: some candidate's first two labels
-    const uint8_t *pre2;    // L^3: some candidate's first three labels
     uint32_t *domains;      // [candidate][position][words]
     uint32_t words;         // ceil(n / 32)
     uint64_t m;             // CSR entries (the (v0, v1) pairs)
@@ -555,13 +553,11 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     // no level has more than L^4 candidates, so a larger buffer would only cost allocation time
     const size_t group_max = std::max<size_t>(1, std::min(budget / per_cand, tsize));
     int32_t *d_table = nullptr;
-    uint8_t *d_pre = nullptr;
     uint32_t *d_dom = nullptr, *d_sizes = nullptr, *d_lc = nullptr;
     uint8_t *d_cands = nullptr;
     unsigned long long *d_queue = nullptr;
     auto release = [&]() {
         cudaFree(d_table);
-        cudaFree(d_pre);
         cudaFree(d_dom);
         cudaFree(d_sizes);
         cudaFree(d_queue);
@@ -569,7 +565,6 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
         cudaFree(d_cands);
     };
     cudaError_t e = cudaMalloc(&d_table, sizeof(int32_t) * tsize);
-    if (e == cudaSuccess) e = cudaMalloc(&d_pre, (size_t)L * L + (size_t)L * L * L);
     if (e == cudaSuccess) e = cudaMalloc(&d_dom, per_cand * group_max);
     if (e == cudaSuccess) e = cudaMalloc(&d_sizes, sizeof(uint32_t) * 4 * group_max);
     if (e == cudaSuccess) e = cudaMalloc(&d_queue, sizeof(unsigned long long));
@@ -588,7 +583,6 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     // the label histogram of every neighbour list (the four-chain and three-star levels)
     if (n > 0) fsm_label_count_kernel<<<grid, 256>>>(gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_lc);
     std::vector<int32_t> table(tsize);
-    std::vector<uint8_t> pre((size_t)L * L + (size_t)L * L * L);
     std::vector<uint8_t> cand_labels(4 * group_max);
     for (int t = kEdge; t <= kThreeStar; ++t) {
         const std::vector<Candidate> cands = candidates_of(t, L, f);
@@ -602,32 +596,25 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
                                                    : &f.star;
         for (size_t g0 = 0; g0 < cands.size(); g0 += group_max) {
             const size_t gn = std::min(group_max, cands.size() - g0);
-            std::fill(table.begin(), table.end(), -1);
-            std::fill(pre.begin(), pre.end(), 0);
-            for (size_t c = 0; c < gn; ++c) {
-                const Labels &lab = cands[g0 + c].canonical;
-                size_t idx = 0;
-                for (int p = 0; p < k; ++p) idx = idx * L + lab[p];
-                table[idx] = (int32_t)c;
-                pre[(size_t)lab[0] * L + lab[1]] = 1;
-                if (k == 4) pre[(size_t)L * L + ((size_t)lab[0] * L + lab[1]) * L + lab[2]] = 1;
-            }
+            // edges and triangles look label tuples up in the dense table; the witness searches read
+            // the candidates' labels directly
+            const bool enumerated = t == kEdge || t == kTriangle;
             size_t tn = 1;
             for (int p = 0; p < k; ++p) tn *= L;
             st = KHZ_OK;
-            if (cudaMemcpy(d_table, table.data(), sizeof(int32_t) * tn, cudaMemcpyHostToDevice) != cudaSuccess ||
-                cudaMemcpy(d_pre, pre.data(), pre.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-                cudaMemset(d_dom, 0, per_cand * gn) != cudaSuccess) {
-                release();
-                return cuda_fail(cudaGetLastError(), "3-FSM tables");
-            }
-            if (cudaMemset(d_queue, 0, sizeof(unsigned long long)) != cudaSuccess) {
-                release();
-                return cuda_fail(cudaGetLastError(), "3-FSM pair counter");
-            }
-            FsmArgs a{gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_table, d_pre, d_pre + (size_t)L * L, d_dom, words,
-                      gi.num_entries, d_queue};
-            if (t == kWedge || k == 4) {
+            if (enumerated) {
+                std::fill(table.begin(), table.begin() + tn, -1);
+                for (size_t c = 0; c < gn; ++c) {
+                    const Labels &lab = cands[g0 + c].canonical;
+                    size_t idx = 0;
+                    for (int p = 0; p < k; ++p) idx = idx * L + lab[p];
+                    table[idx] = (int32_t)c;
+                }
+                if (cudaMemcpy(d_table, table.data(), sizeof(int32_t) * tn, cudaMemcpyHostToDevice) != cudaSuccess) {
+                    release();
+                    return cuda_fail(cudaGetLastError(), "3-FSM tables");
+                }
+            } else {
                 for (size_t c = 0; c < gn; ++c)
                     for (int p = 0; p < 4; ++p)
                         cand_labels[4 * c + p] = p < k ? (uint8_t)cands[g0 + c].canonical[p] : (uint8_t)0;
@@ -636,6 +623,12 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
                     return cuda_fail(cudaGetLastError(), "3-FSM candidates");
                 }
             }
+            if (cudaMemset(d_dom, 0, per_cand * gn) != cudaSuccess ||
+                cudaMemset(d_queue, 0, sizeof(unsigned long long)) != cudaSuccess) {
+                release();
+                return cuda_fail(cudaGetLastError(), "3-FSM domains and claim counter");
+            }
+            FsmArgs a{gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_table, d_dom, words, gi.num_entries, d_queue};
             FsmExistArgs x{gi.d_offsets, gi.d_adj, gi.d_labels, d_lc, n, L, d_cands, (uint32_t)gn, d_dom, words, d_queue};
             const int xgrid = sms * 8;
             switch (t) {
