@@ -878,3 +878,237 @@ uint64_t orc_brute(int pattern, uint32_t n, const uint64_t *off, const uint32_t 
     }
     return total;
 }
+
+/* ------------------------------------------------------------------------- */
+/* 3-FSM (kautomine/three_fsm.cc)                                            */
+/* ------------------------------------------------------------------------- */
+
+/* Neighbour lists regrouped by label: the label-l neighbours of v are
+ * ladj[loff[v * L + l] .. loff[v * L + l + 1]), ascending ids (the CSR order kept). */
+typedef struct {
+    uint32_t n, L;
+    uint64_t *loff;
+    uint32_t *ladj;
+    const uint32_t *labels;
+    uint8_t *dom[4]; /* per pattern position: 1 where some embedding maps a vertex there */
+} orc_fsm_graph;
+
+static const uint32_t *fsm_nbrs(const orc_fsm_graph *g, uint32_t v, uint32_t l, uint32_t *len) {
+    const uint64_t b = g->loff[(uint64_t)v * g->L + l];
+    *len = (uint32_t)(g->loff[(uint64_t)v * g->L + l + 1] - b);
+    return g->ladj + b;
+}
+
+static void fsm_mark(const orc_fsm_graph *g, int pos, uint32_t v) {
+    __atomic_store_n(&g->dom[pos][v], (uint8_t)1, __ATOMIC_RELAXED);
+}
+
+/* The images of the pairs (a, b), a in A \ {skip_a}, b in B \ {skip_b}, a != b, at positions
+ * pa and pb (the last two vertices of a wedge, four-chain or three-star, which the app's loops
+ * pick independently under exactly these exclusions).  a has a partner iff B holds a vertex
+ * other than skip_b and a; likewise b.  Returns whether any pair exists. */
+static int fsm_pair_images(const orc_fsm_graph *g, const uint32_t *A, uint32_t na, uint32_t skip_a,
+                           const uint32_t *B, uint32_t nb, uint32_t skip_b, int pa, int pb) {
+    uint32_t ea = 0, eb = 0, a1 = 0, b1 = 0;
+    for (uint32_t i = 0; i < na; ++i) if (A[i] != skip_a) { if (ea == 0) a1 = A[i]; ea++; }
+    for (uint32_t i = 0; i < nb; ++i) if (B[i] != skip_b) { if (eb == 0) b1 = B[i]; eb++; }
+    int any = 0;
+    for (uint32_t i = 0; i < na; ++i) {
+        const uint32_t a = A[i];
+        if (a == skip_a) continue;
+        if (eb >= 2 || (eb == 1 && b1 != a)) { fsm_mark(g, pa, a); any = 1; }
+    }
+    for (uint32_t i = 0; i < nb; ++i) {
+        const uint32_t b = B[i];
+        if (b == skip_b) continue;
+        if (ea >= 2 || (ea == 1 && a1 != b)) fsm_mark(g, pb, b);
+    }
+    return any;
+}
+
+enum { FSM_EDGE = 0, FSM_WEDGE = 1, FSM_TRIANGLE = 2, FSM_FOUR_CHAIN = 3, FSM_THREE_STAR = 4 };
+
+/* The embeddings one candidate's run inserts with enable = true (three_fsm.cc:53-262), started
+ * from the vertices whose label is c[0] (run(true, true, labels[0]), three_fsm.cc:606):
+ *   edge        v1 in N(v0)                                      (53-68)
+ *   wedge       v1, v2 in N(v0), v2 != v1                        (69-107)
+ *   triangle    v1 in N(v0), v2 in N(v0) n N(v1)                 (108-151)
+ *   four-chain  v1, v2 in N(v0), v2 != v1; v3 in N(v1) \ {v0, v2} (152-200)
+ *   three-star  v1 in N(v0); v2 in N(v1) \ {v0}; v3 in N(v1) \ {v0, v2} (201-250)
+ * each with its vertices' labels equal to c.  The images per position are marked per (v0) or
+ * (v0, v1) prefix without listing the last two vertices' pairs one by one. */
+static void fsm_domains(const orc_fsm_graph *g, int t, const uint32_t *c, int threads) {
+    const uint32_t n = g->n;
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 64)
+    for (uint32_t v0 = 0; v0 < n; ++v0) {
+        if (g->labels[v0] != c[0]) continue;
+        uint32_t n1;
+        const uint32_t *N1 = fsm_nbrs(g, v0, c[1], &n1);
+        if (t == FSM_EDGE) {
+            if (n1) fsm_mark(g, 0, v0);
+            for (uint32_t i = 0; i < n1; ++i) fsm_mark(g, 1, N1[i]);
+            continue;
+        }
+        if (t == FSM_WEDGE) {
+            uint32_t n2;
+            const uint32_t *N2 = fsm_nbrs(g, v0, c[2], &n2);
+            if (fsm_pair_images(g, N1, n1, UINT32_MAX, N2, n2, UINT32_MAX, 1, 2)) fsm_mark(g, 0, v0);
+            continue;
+        }
+        for (uint32_t i = 0; i < n1; ++i) {
+            const uint32_t v1 = N1[i];
+            int any = 0;
+            if (t == FSM_TRIANGLE) {
+                uint32_t na, nb;
+                const uint32_t *A = fsm_nbrs(g, v0, c[2], &na), *B = fsm_nbrs(g, v1, c[2], &nb);
+                for (uint32_t x = 0, y = 0; x < na && y < nb;) {
+                    if (A[x] < B[y]) ++x;
+                    else if (A[x] > B[y]) ++y;
+                    else { fsm_mark(g, 2, A[x]); any = 1; ++x; ++y; }
+                }
+            } else if (t == FSM_FOUR_CHAIN) {
+                uint32_t na, nb;
+                const uint32_t *A = fsm_nbrs(g, v0, c[2], &na), *B = fsm_nbrs(g, v1, c[3], &nb);
+                any = fsm_pair_images(g, A, na, v1, B, nb, v0, 2, 3);
+            } else {
+                uint32_t na, nb;
+                const uint32_t *A = fsm_nbrs(g, v1, c[2], &na), *B = fsm_nbrs(g, v1, c[3], &nb);
+                any = fsm_pair_images(g, A, na, v0, B, nb, v0, 2, 3);
+            }
+            if (any) { fsm_mark(g, 0, v0); fsm_mark(g, 1, v1); }
+        }
+    }
+}
+
+/* Candidate labellings of one level (CandidateLabeledPatternGenerator, three_fsm.cc:315-590), in
+ * the generator's loop order.  fv / fe / fw: frequent vertex labels, edges (L^2) and wedges (L^3).
+ * cand receives 4 labels per candidate (canonical order); returns the number of candidates. */
+static uint32_t fsm_candidates(int t, uint32_t L, const uint8_t *fv, const uint8_t *fe, const uint8_t *fw,
+                               uint32_t *cand) {
+    uint32_t nc = 0;
+#define FE(a, b) fe[(a) * L + (b)]
+#define FW(a, b, c) fw[((a) * L + (b)) * L + (c)]
+#define PUT(a, b, c, d) do { cand[4 * nc] = (a); cand[4 * nc + 1] = (b); cand[4 * nc + 2] = (c); \
+                             cand[4 * nc + 3] = (d); nc++; } while (0)
+    for (uint32_t l0 = 0; l0 < L; ++l0) {
+        if (!fv[l0]) continue;
+        for (uint32_t l1 = 0; l1 < L; ++l1) {
+            if (t == FSM_EDGE) { /* 315-343 */
+                if (fv[l1] && l0 <= l1) PUT(l0, l1, 0, 0);
+                continue;
+            }
+            if (!FE(l0, l1)) continue;
+            for (uint32_t l2 = 0; l2 < L; ++l2) {
+                if (t == FSM_WEDGE) { /* 345-389 */
+                    if (FE(l0, l2) && l1 <= l2) PUT(l0, l1, l2, 0);
+                    continue;
+                }
+                if (!FW(l0, l1, l2)) continue;
+                if (t == FSM_TRIANGLE) { /* 391-452 */
+                    if (FW(l1, l0, l2) && FW(l2, l0, l1) && l0 <= l1 && l1 <= l2) PUT(l0, l1, l2, 0);
+                    continue;
+                }
+                for (uint32_t l3 = 0; l3 < L; ++l3) {
+                    if (t == FSM_FOUR_CHAIN) { /* 454-512 */
+                        if (FW(l1, l0, l3) && FE(l0, l2) && FE(l1, l3) && l0 <= l1) PUT(l0, l1, l2, l3);
+                    } else { /* 514-589: the centre's label l0 goes second */
+                        if (FW(l0, l2, l3) && FW(l0, l1, l3) && l1 <= l2 && l2 <= l3) PUT(l1, l0, l2, l3);
+                    }
+                }
+            }
+        }
+    }
+#undef FE
+#undef FW
+#undef PUT
+    return nc;
+}
+
+int orc_fsm(uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *labels, uint32_t L,
+            uint32_t threshold, int threads, uint32_t *num_candidates, uint32_t *num_frequent,
+            uint64_t *support_sum) {
+    if (L == 0 || L > ORC_FSM_MAX_LABELS) return -1;
+    for (uint32_t v = 0; v < n; ++v) if (labels[v] >= L) return -1;
+    if (threads <= 0) threads = omp_get_max_threads();
+    const uint64_t m = off[n];
+    orc_fsm_graph g;
+    memset(&g, 0, sizeof(g));
+    g.n = n;
+    g.L = L;
+    g.labels = labels;
+    g.loff = (uint64_t *)calloc((size_t)n * L + 1, sizeof(uint64_t));
+    g.ladj = (uint32_t *)malloc(sizeof(uint32_t) * (m ? m : 1));
+    const size_t L4 = (size_t)L * L * L * L;
+    uint8_t *fe = (uint8_t *)calloc((size_t)L * L, 1), *fw = (uint8_t *)calloc((size_t)L * L * L, 1);
+    uint32_t *cand = (uint32_t *)malloc(sizeof(uint32_t) * 4 * L4);
+    uint8_t fv[ORC_FSM_MAX_LABELS] = {0};
+    int rc = g.loff && g.ladj && fe && fw && cand ? 0 : -1;
+    for (int p = 0; p < 4 && rc == 0; ++p) if (!(g.dom[p] = (uint8_t *)malloc(n ? n : 1))) rc = -1;
+    if (rc == 0) {
+        /* regroup every list by label: a counting pass, then a stable scatter */
+        for (uint32_t v = 0; v < n; ++v)
+            for (uint64_t e = off[v]; e < off[v + 1]; ++e) g.loff[(uint64_t)v * L + labels[adj[e]] + 1]++;
+        for (uint64_t i = 0; i < (uint64_t)n * L; ++i) g.loff[i + 1] += g.loff[i];
+        uint64_t *fill = (uint64_t *)malloc(sizeof(uint64_t) * ((size_t)n * L + 1));
+        if (!fill) rc = -1;
+        else {
+            memcpy(fill, g.loff, sizeof(uint64_t) * ((size_t)n * L + 1));
+            for (uint32_t v = 0; v < n; ++v)
+                for (uint64_t e = off[v]; e < off[v + 1]; ++e) g.ladj[fill[(uint64_t)v * L + labels[adj[e]]]++] = adj[e];
+            free(fill);
+        }
+    }
+    if (rc == 0) {
+        /* level 0, setup (three_fsm.cc:289-310): every label's vertex count enters the sum */
+        uint64_t per[ORC_FSM_MAX_LABELS] = {0};
+        for (uint32_t v = 0; v < n; ++v) per[labels[v]]++;
+        num_candidates[0] = L;
+        num_frequent[0] = 0;
+        support_sum[0] = 0;
+        for (uint32_t l = 0; l < L; ++l) {
+            fv[l] = per[l] >= threshold;
+            num_frequent[0] += fv[l];
+            support_sum[0] += per[l];
+        }
+        static const int kSize[5] = {2, 3, 3, 4, 4};
+        for (int t = FSM_EDGE; t <= FSM_THREE_STAR; ++t) {
+            const uint32_t nc = fsm_candidates(t, L, fv, fe, fw, cand);
+            const int k = kSize[t];
+            /* the next levels read this level's frequent set: edges and wedges only */
+            uint8_t *freq = t == FSM_EDGE ? fe : t == FSM_WEDGE ? fw : NULL;
+            num_candidates[1 + t] = nc;
+            num_frequent[1 + t] = 0;
+            support_sum[1 + t] = 0;
+            for (uint32_t ci = 0; ci < nc; ++ci) {
+                const uint32_t *c = cand + 4 * ci;
+                for (int p = 0; p < 4; ++p) memset(g.dom[p], 0, n);
+                fsm_domains(&g, t, c, threads);
+                /* get_support (engine.h:384-401): the least image count, starting from n */
+                uint32_t support = n;
+                for (int p = 0; p < k; ++p) {
+                    uint32_t s = 0;
+                    for (uint32_t v = 0; v < n; ++v) s += g.dom[p][v];
+                    if (s < support) support = s;
+                }
+                if (support < threshold) continue;
+                num_frequent[1 + t]++;
+                support_sum[1 + t] += support;
+                /* the canonical labelling and its automorphisms join the frequent set */
+                if (t == FSM_EDGE) {
+                    freq[c[0] * L + c[1]] = 1;
+                    freq[c[1] * L + c[0]] = 1;
+                } else if (t == FSM_WEDGE) {
+                    freq[(c[0] * L + c[1]) * L + c[2]] = 1;
+                    freq[(c[0] * L + c[2]) * L + c[1]] = 1;
+                }
+            }
+        }
+    }
+    for (int p = 0; p < 4; ++p) free(g.dom[p]);
+    free(g.loff);
+    free(g.ladj);
+    free(fe);
+    free(fw);
+    free(cand);
+    return rc;
+}

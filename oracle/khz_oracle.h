@@ -98,6 +98,19 @@ int orc_count_labeled(int app, uint32_t n, const uint64_t *off, const uint32_t *
  * 10..15 induced 4-motifs in the order 3-star, 4-path, tailed triangle, 4-cycle, diamond, 4-clique. */
 uint64_t orc_brute(int pattern, uint32_t n, const uint64_t *off, const uint32_t *adj);
 
+/* ---- 3-FSM (kautomine/three_fsm.cc:53-800) ----
+ * The app's level driver on a symmetric labelled graph (labels dense in [0, L), L <= 48 as
+ * MAX_NUM_LABELS, graph_loader.h:28): levels 0 single vertices, 1 edges, 2 wedges, 3 triangles,
+ * 4 four-chains, 5 three-stars, each level's candidates generated from the frequent patterns before
+ * it (three_fsm.cc:315-590) and each candidate's MNI support the least number of distinct vertices
+ * its embeddings map to one position (engine.h:384-401).  Fills, per level, the number of
+ * candidates, of frequent patterns (support >= threshold) and their support sum (level 0: the sum
+ * over every label, as setup() prints it).  Returns 0, or -1 for bad labels or no memory. */
+#define ORC_FSM_MAX_LABELS 48
+int orc_fsm(uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *labels, uint32_t L,
+            uint32_t threshold, int threads, uint32_t *num_candidates, uint32_t *num_frequent,
+            uint64_t *support_sum);
+
 #ifdef __cplusplus
 }
 #endif

@@ -97,6 +97,9 @@ def lib():
                                         ctypes.POINTER(ctypes.c_uint64)]
         L.orc_brute.restype = ctypes.c_uint64
         L.orc_brute.argtypes = [ctypes.c_int, ctypes.c_uint32, _u64p, _u32p]
+        L.orc_fsm.restype = ctypes.c_int
+        L.orc_fsm.argtypes = [ctypes.c_uint32, _u64p, _u32p, _u32p, ctypes.c_uint32, ctypes.c_uint32,
+                              ctypes.c_int, _u32p, _u32p, _u64p]
         _lib = L
     return _lib
 
@@ -252,3 +255,24 @@ def run_reference(app, dgraph, threads=-1, runs=1, label=None, timeout=3600):
             if line.strip().startswith("NumExtensions"):
                 ext = line
     return [counts[k] for k in sorted(counts)], rt, ext
+
+
+def fsm(off, adj, labels, threshold, threads=0):
+    """The 3-FSM levels (kautomine/three_fsm.cc) of a symmetric labelled graph: per level (single
+    vertices, edges, wedges, triangles, four-chains, three-stars) a dict with num_candidates,
+    num_frequent and support_sum."""
+    labels = np.ascontiguousarray(labels, dtype=np.uint32)
+    n = off.shape[0] - 1
+    nl = int(labels.max()) + 1 if n else 1
+    nc = np.zeros(6, dtype=np.uint32)
+    nf = np.zeros(6, dtype=np.uint32)
+    ss = np.zeros(6, dtype=np.uint64)
+    adj = np.ascontiguousarray(adj, dtype=np.uint32)
+    if adj.shape[0] == 0:
+        adj = np.zeros(1, dtype=np.uint32)
+    rc = lib().orc_fsm(n, off, adj, labels if n else np.zeros(1, dtype=np.uint32), nl, threshold, threads,
+                       nc, nf, ss)
+    if rc != 0:
+        raise ValueError("orc_fsm failed (%d)" % rc)
+    return [{"num_candidates": int(nc[i]), "num_frequent": int(nf[i]), "support_sum": int(ss[i])}
+            for i in range(6)]
