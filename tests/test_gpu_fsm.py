@@ -66,3 +66,36 @@ def test_fsm_needs_symmetric_graph(khz_ctx):
         assert e.value.status == 1
     finally:
         g.free()
+
+
+def _skewed_labels(n, num_labels, mult=7919):
+    """label l with weight l + 1, spread over the ids by a multiplier coprime to the weight sum"""
+    r = (np.arange(n, dtype=np.uint64) * mult) % (num_labels * (num_labels + 1) // 2)
+    return np.searchsorted(np.cumsum(np.arange(1, num_labels + 1)), r, side="right").astype(np.uint32)
+
+
+# (scale, edge factor, labels, threshold divisor): thresholds n // divisor prune some candidates at
+# every level; up to 4 608 four-chain candidates (12 labels)
+_ORACLE_CASES = [(14, 16, 2, 3), (14, 16, 3, 4), (14, 16, 5, 6), (14, 16, 8, 10), (14, 16, 8, 40),
+                 (13, 16, 12, 60), (15, 8, 4, 5)]
+
+
+def test_fsm_matches_oracle_on_larger_graphs(khz_ctx):
+    """The device's levels (candidates, frequent patterns, support sums) against the oracle's
+    restatement (orc_fsm) on labelled R-MAT graphs of 6 500 to 21 000 vertices with skewed labels."""
+    import orc
+    for scale, ef, num_labels, div in _ORACLE_CASES:
+        canon, n = orc.rmat(scale, ef, seed=11)
+        sym = orc.symmetrize(canon)
+        off, adj = orc.csr(sym, n)
+        labels = _skewed_labels(n, num_labels)
+        threshold = max(1, n // div)
+        want = orc.fsm(off, adj, labels, threshold)
+        g = khz_ctx.graph_from_edges(sym, n)
+        try:
+            g.set_labels(labels)
+            got, _, _ = khz_ctx.fsm(g, threshold)
+        finally:
+            g.free()
+        assert [(x["num_candidates"], x["num_frequent"], x["support_sum"]) for x in got] == \
+            [(x["num_candidates"], x["num_frequent"], x["support_sum"]) for x in want], (scale, ef, num_labels, div)
