@@ -10,11 +10,12 @@
 // support is the least of these (get_support, engine.h:384-401).
 //
 // Where the reference runs the engine once per candidate (run(..., restrict_starting_vertex_label,
-// labels[0])), the device answers all of a level's candidates at once.  Edges and triangles: every
-// embedding of the level's template is enumerated once (a warp per v0, or per (v0, v1) pair with
-// lanes over the last vertex), and an embedding whose label tuple is a candidate (one lookup in a
-// dense table indexed by the labels) sets its vertices' bits in that candidate's per-position domain
-// bitmaps (a word is read before the atomicOr, so repeated images cost no atomics).  Wedges,
+// labels[0])), the device answers all of a level's candidates at once.  Edges: every embedding is
+// enumerated once (a warp per v0); triangles: each is listed once, from its lowest vertex in
+// (degree, id) order (a warp per (v0, v1) pair, lanes over v2), and its six vertex orders are the
+// embeddings.  An embedding whose label tuple is a candidate (one lookup in a dense table indexed by
+// the labels) sets its vertices' bits in that candidate's per-position domain bitmaps (a word is
+// read before the atomicOr, so repeated images cost no atomics).  Wedges,
 // four-chains and three-stars, whose embeddings are far more numerous: each (candidate, position,
 // vertex) is decided by a search for one witness embedding over label counts of the neighbour lists
 // (see below).  A
