@@ -3,7 +3,7 @@ unmodified into oracle/_ref/kautomine_three_fsm by oracle/Makefile) on seeded la
 For each (graph, threshold) it records the lines the app prints per level: the number of frequent
 patterns and their support sum.
 
-    python tests/golden/make_fsm_golden.py      # about a minute on 8 cores
+    python tests/golden/make_fsm_golden.py      # about 13 minutes on 8 cores
 """
 import json
 import os
@@ -31,6 +31,20 @@ GRAPHS = [
     # two labels: patterns with equal labels on symmetric positions, hubs of degree ~300
     {"name": "rmat_s11_ef8_s4_l2", "kind": "rmat", "scale": 11, "ef": 8, "seed": 4, "labels": 2, "mult": 3,
      "thresholds": [100, 400]},
+    # skewed labels (label l with weight l + 1): thresholds that prune candidates at every level,
+    # up to 12 labels (4 608 four-chain candidates)
+    {"name": "rmat_s14_ef16_s11_skew2", "kind": "rmat", "scale": 14, "ef": 16, "seed": 11, "labels": 2,
+     "mult": 7919, "rule": "skew", "thresholds": [4181]},
+    {"name": "rmat_s14_ef16_s11_skew3", "kind": "rmat", "scale": 14, "ef": 16, "seed": 11, "labels": 3,
+     "mult": 7919, "rule": "skew", "thresholds": [3136]},
+    {"name": "rmat_s14_ef16_s11_skew5", "kind": "rmat", "scale": 14, "ef": 16, "seed": 11, "labels": 5,
+     "mult": 7919, "rule": "skew", "thresholds": [2090]},
+    {"name": "rmat_s14_ef16_s11_skew8", "kind": "rmat", "scale": 14, "ef": 16, "seed": 11, "labels": 8,
+     "mult": 7919, "rule": "skew", "thresholds": [1254, 313]},
+    {"name": "rmat_s13_ef16_s11_skew12", "kind": "rmat", "scale": 13, "ef": 16, "seed": 11, "labels": 12,
+     "mult": 7919, "rule": "skew", "thresholds": [108]},
+    {"name": "rmat_s15_ef8_s11_skew4", "kind": "rmat", "scale": 15, "ef": 8, "seed": 11, "labels": 4,
+     "mult": 7919, "rule": "skew", "thresholds": [4213]},
 ]
 
 LEVELS = ["single-vertex", "single-edge", "wedge", "triangle", "four-chain", "three-star"]
@@ -42,7 +56,13 @@ def graph_of(spec):
         canon, n = orc.er(spec["n"], spec["m"], spec["seed"])
     else:
         canon, n = orc.rmat(spec["scale"], spec["ef"], seed=spec["seed"])
-    labels = (np.arange(n, dtype=np.uint64) * spec["mult"] % spec["labels"]).astype(np.uint32)
+    if spec.get("rule", "mod") == "skew":
+        # label l with weight l + 1: the residue of v * mult modulo L(L+1)/2 picks the label
+        nl = spec["labels"]
+        r = np.arange(n, dtype=np.uint64) * spec["mult"] % (nl * (nl + 1) // 2)
+        labels = np.searchsorted(np.cumsum(np.arange(1, nl + 1)), r, side="right").astype(np.uint32)
+    else:
+        labels = (np.arange(n, dtype=np.uint64) * spec["mult"] % spec["labels"]).astype(np.uint32)
     return orc.symmetrize(canon), n, labels
 
 

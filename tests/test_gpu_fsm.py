@@ -75,17 +75,18 @@ def _skewed_labels(n, num_labels, mult=7919):
 
 
 # (scale, edge factor, labels, threshold divisor): thresholds n // divisor prune some candidates at
-# every level; up to 4 608 four-chain candidates (12 labels)
+# every level; up to 4 272 four-chain candidates (12 labels).  Seed 12: the golden fixture holds the
+# reference's own results for the same shapes on seed 11.
 _ORACLE_CASES = [(14, 16, 2, 3), (14, 16, 3, 4), (14, 16, 5, 6), (14, 16, 8, 10), (14, 16, 8, 40),
-                 (13, 16, 12, 60), (15, 8, 4, 5)]
+                 (13, 16, 12, 60), (15, 8, 4, 5), (16, 8, 6, 12)]
 
 
 def test_fsm_matches_oracle_on_larger_graphs(khz_ctx):
     """The device's levels (candidates, frequent patterns, support sums) against the oracle's
-    restatement (orc_fsm) on labelled R-MAT graphs of 6 500 to 21 000 vertices with skewed labels."""
+    restatement (orc_fsm) on labelled R-MAT graphs of 6 500 to 40 000 vertices with skewed labels."""
     import orc
     for scale, ef, num_labels, div in _ORACLE_CASES:
-        canon, n = orc.rmat(scale, ef, seed=11)
+        canon, n = orc.rmat(scale, ef, seed=12)
         sym = orc.symmetrize(canon)
         off, adj = orc.csr(sym, n)
         labels = _skewed_labels(n, num_labels)
