@@ -213,23 +213,26 @@ def labelled_oriented_dgraph(g, tmpdir):
     return path
 
 
-def run_reference_sample(dgraph, runs):
+def run_reference_sample(dgraph, runs, warmup=0):
     """The reference's own kautomine four_clique (apply + engine, compiled unmodified) over the
-    start vertices of label class 0.  Returns a dict: per-run seconds, embeddings, count and
-    NumExtensions per run, kind ("reference" or "port"), threads used."""
+    start vertices of label class 0, `warmup` untimed runs first.  Returns a dict: per-run seconds,
+    embeddings, count and NumExtensions per run, kind ("reference" or "port"), threads used."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
     logical = os.cpu_count() or 1
     exe = os.path.join(orc.REF_DIR, "sample_" + APP)
     if os.path.exists(exe):
-        counts, avg_ms, ext = orc.run_reference(APP, dgraph, threads=-1, runs=runs, label=0, timeout=3000)
-        per_run_ext = ext // runs
+        counts, avg_ms, ext = orc.run_reference(APP, dgraph, threads=-1, runs=runs, label=0, timeout=3000,
+                                                warmup=warmup)
+        per_run_ext = ext // (runs + warmup)
         threads = max(1, logical - 2)  # the reference caps compute threads at CPUs - 2 (distributed_application.cc:80)
         return {"secs": avg_ms / 1000.0, "embeddings": per_run_ext + counts[0], "count": counts[0],
                 "num_extensions": per_run_ext, "kind": "reference", "threads": threads}
     # the oracle port (C restatement) when the reference binaries are not present
     n, pairs, _ = orc.read_dgraph(dgraph)
     off, adj = orc.csr(pairs, n)
+    for _ in range(warmup):
+        orc.count(APP, off, adj, v0_mod=SAMPLE_MOD, v0_rem=0, threads=logical)
     t0 = time.time()
     for _ in range(runs):
         counts, ext, _ = orc.count(APP, off, adj, v0_mod=SAMPLE_MOD, v0_rem=0, threads=logical)
@@ -374,7 +377,7 @@ def ours(args, rank, world, local):
         import numpy as np
         with tempfile.TemporaryDirectory() as td:
             path = labelled_oriented_dgraph(g, td)
-            r = run_reference_sample(path, runs=1)
+            r = run_reference_sample(path, runs=1, warmup=1)
         # the same slice on the device (restrict_starting_vertex_label): the reference's count and
         # NumExtensions must be the device's
         g.set_labels((np.arange(n, dtype=np.uint64) % SAMPLE_MOD).astype(np.uint32))
@@ -849,11 +852,11 @@ def reference_arm(args, rank, world, local):
             orc.write_dgraph(path, n, np.stack([src, oadj], axis=1),
                              (np.arange(n, dtype=np.uint64) % SAMPLE_MOD).astype(np.uint32))
         t_build = time.time() - t0
-        r = run_reference_sample(path, runs=args.steps)
+        r = run_reference_sample(path, runs=args.steps, warmup=args.warmup)
     value = r["embeddings"] / r["secs"]
     model, cores, logical = host_cpu()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "embeddings/s", "n_gpus": 0,
-            "steps": args.steps, "warmup": 0, "ms_per_step": r["secs"] * 1000.0, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["secs"] * 1000.0, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic",
             "config": {"workload": workload_name(args.scale, args.edge_factor), "sample": "v0 %% %d == 0" % SAMPLE_MOD,
                        "same_config": False,

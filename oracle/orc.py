@@ -228,17 +228,19 @@ _RT_RE = re.compile(r"Average runtime: ([0-9.]+) \(ms\)")
 _EXT_RE = re.compile(r"NumExtensionsTotal: ([0-9.]+)")
 
 
-def run_reference(app, dgraph, threads=-1, runs=1, label=None, timeout=3600):
+def run_reference(app, dgraph, threads=-1, runs=1, label=None, timeout=3600, warmup=0):
     """Run the reference's own app binary from oracle/_ref.  With label=None the stock
     app runs on the whole graph; with a label the sampled driver runs the v0 slice whose
-    on-disk node label equals it.  Returns (counts, average runtime ms, num_extensions or None)."""
+    on-disk node label equals it, after `warmup` untimed runs.  Returns (counts, average runtime
+    ms of the timed runs, num_extensions or None; the sampled driver's is the total over all runs,
+    warm-up runs included)."""
     env = dict(os.environ)
     if label is None:
         exe = os.path.join(REF_DIR, app)
         args = [exe, dgraph, str(threads), str(runs), "false"]
     else:
         exe = os.path.join(REF_DIR, "sample_" + app)
-        args = [exe, dgraph, str(threads), str(label), str(runs)]
+        args = [exe, dgraph, str(threads), str(label), str(runs)] + ([str(warmup)] if warmup > 0 else [])
     out = subprocess.run(args, capture_output=True, text=True, timeout=timeout, env=env)
     if out.returncode != 0:
         raise RuntimeError("%s failed (%d): %s" % (exe, out.returncode, out.stderr[-2000:]))

@@ -9,22 +9,25 @@
 // .dgraph whose node labels are v % S this processes one S-th slice of the start
 // vertices: a bounded, reproducible sample of the full workload.
 //
-// usage: sample_<app> <labeled graph.dgraph> <num_threads|-1> <label> <runs>
-// prints the reference's own lines: "Pattern count <i>: <n>" and "Average runtime: <ms> (ms)",
-// plus "NumExtensionsTotal: <n>" (the engine's NumExtensions accumulated over all runs).
+// usage: sample_<app> <labeled graph.dgraph> <num_threads|-1> <label> <runs> [warm-up runs]
+// prints the reference's own lines: "Pattern count <i>: <n>" and "Average runtime: <ms> (ms)" (over
+// the timed runs, which follow the untimed warm-up runs), plus "NumExtensionsTotal: <n>" (the
+// engine's NumExtensions accumulated over all runs, warm-up runs included).
 #define main khz_reference_app_main
 #include KHZ_APP_SRC
 #undef main
 
 int main(int argc, char **argv) {
-    if (argc != 5) {
-        fprintf(stderr, "usage: %s <labeled graph.dgraph> <num_threads|-1> <label> <runs>\n", argv[0]);
+    if (argc != 5 && argc != 6) {
+        fprintf(stderr, "usage: %s <labeled graph.dgraph> <num_threads|-1> <label> <runs> [warm-up runs]\n",
+                argv[0]);
         return 2;
     }
     DistributedSys::init_distributed_sys();
     int num_threads = std::atoi(argv[2]);
     LabelId label = (LabelId)std::atoi(argv[3]);
     int runs = std::atoi(argv[4]);
+    int warmup = argc == 6 ? std::atoi(argv[5]) : 0;
     Khuzdul::DistributedApplication *app = new Khuzdul::DistributedApplication(
         num_threads, std::string(argv[1]), MAX_COUNTING_PATTERN_SIZE, Khuzdul::apply, true);
 #ifndef ENABLE_COMPUTE_FUSION
@@ -35,7 +38,8 @@ int main(int argc, char **argv) {
     Khuzdul::LocalPerformanceMetric::init_local_metrics();
     double average_runtime = 0;
     EdgeId cnt[NUM_COUNTING_PATTERNS];
-    for (int run = 0; run < runs; ++run) {
+    for (int run = -warmup; run < runs; ++run) {
+        if (run == 0) average_runtime = 0;  // the warm-up runs are not timed
         average_runtime -= get_time();
 #ifndef ENABLE_COMPUTE_FUSION
         for (int p = 0; p < NUM_COUNTING_PATTERNS; ++p) {
