@@ -63,3 +63,22 @@ def test_bench_reads_kernel_traffic_from_the_profile():
     got = {k: bench.profile_traffic(k) for k in khz.Stats.PHASES[:3]}
     assert all(isinstance(v, int) and v > 0 for v in got.values()), got
     assert bench.profile_traffic("no_such_kernel") is None
+
+
+def test_clock_summary_reads_nvidia_smi_lines():
+    """The clocks object of the bench line: the median SM clock under load, the highest max clock and
+    the throttle reasons seen active (nvidia-smi csv, noheader, nounits)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.ClockSampler(0)
+    c.lines = ["1965, 1965, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+               "1950, 1965, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+               "1900, 1965, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+               "[N/A], 1965, garbage",
+               ""]
+    s = c.summary()
+    assert s == {"sm_mhz": 1950.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    c.lines = ["1300, 1965, 0x0000000000000048, Active, Not Active, Active, Not Active"]
+    assert c.summary()["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
+    c.lines = []
+    assert c.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
