@@ -544,15 +544,16 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
         out->level[0].support_sum += per_label[l];
         if (f.vertex[l]) emit(0, {l}, (uint32_t)per_label[l]);
     }
-    // device buffers for the label tables (sized for L^4) and the domains (grouped by budget)
-    const size_t tsize = (size_t)L * L * L * L;
+    // device buffers: the label-tuple table of the edge and triangle levels (L^3 entries) and the
+    // domains (grouped by budget)
+    const size_t tsize = (size_t)L * L * L;
     const uint32_t words = (n + 31) / 32;
     size_t free_b = 0, total_b = 0;
     KHZ_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t budget = std::max<size_t>(free_b / 4, (size_t)64 << 20);
     const size_t per_cand = (size_t)4 * words * sizeof(uint32_t);
     // no level has more than L^4 candidates, so a larger buffer would only cost allocation time
-    const size_t group_max = std::max<size_t>(1, std::min(budget / per_cand, tsize));
+    const size_t group_max = std::max<size_t>(1, std::min(budget / per_cand, tsize * L));
     int32_t *d_table = nullptr;
     uint32_t *d_dom = nullptr, *d_sizes = nullptr, *d_lc = nullptr;
     uint8_t *d_cands = nullptr;
@@ -581,7 +582,7 @@ extern "C" khz_status khz_fsm(khz_ctx *ctx, khz_graph g, uint32_t threshold, khz
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(((uint64_t)n + 7) / 8, (uint64_t)sms * 16));
-    // the label histogram of every neighbour list (the four-chain and three-star levels)
+    // the label histogram of every neighbour list (the wedge, four-chain and three-star levels)
     if (n > 0) fsm_label_count_kernel<<<grid, 256>>>(gi.d_offsets, gi.d_adj, gi.d_labels, n, L, d_lc);
     std::vector<int32_t> table(tsize);
     std::vector<uint8_t> cand_labels(4 * group_max);
