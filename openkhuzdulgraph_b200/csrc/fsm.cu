@@ -273,8 +273,8 @@ __device__ __forceinline__ void set_domain_bit(const FsmExistArgs &a, uint32_t c
 
 // The positions p of candidate c (labels c0..c3) that x, with label lx, could take: cl[p] == lx and
 // x's own label counts allow the position (necessary conditions of the searches below, so a
-// position dropped here has no witness).  The three-star centre needs only x's label counts and is
-// decided here outright.
+// position dropped here has no witness).  The wedge centre and the three-star centre need only x's
+// label counts and are decided here outright.
 template <int T>
 __device__ __forceinline__ unsigned open_positions(const FsmExistArgs &a, uint32_t c, uint32_t x, uint32_t lx,
                                                    uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3) {
